@@ -1,0 +1,251 @@
+// pearl_device.cuh — device-side building blocks of the FP64 hot path.
+//
+// Pointwise thermodynamics and kinetics follow pearl_serial.cpp with the same
+// floating-point operation order; the translation unit is compiled with
+// -fmad=false, so a multiply followed by an add is never fused unless the
+// reference itself calls std::fma.  Per-cell results are therefore bitwise
+// equal to the reference's; only global sums (CG dot products, carbon mass,
+// energy) differ, because they are reduced as a fixed-order tree instead of a
+// sequential row-major loop.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pearl_gpu.h"
+
+namespace pearl_gpu {
+
+constexpr int kTileX = 32;  // one warp spans 32 consecutive x cells (256 B of a row)
+constexpr int kTileY = 8;   // 8 warps stack 8 rows
+constexpr int kThreads = kTileX * kTileY;
+constexpr int kMaxRed = 6;  // values per grid reduction
+
+// Device copy of pearl_params plus host-precomputed constants.  Each constant
+// is evaluated on the host with the reference's own expression, so its bits
+// equal what the reference recomputes per cell.
+struct DevParams {
+    int nx, ny, pitch, ntx, nty, ntiles;
+    double dx, dy, dx2, dy2;
+    double Vm, eps, obs, tr, two_eps_sigma, eps_sigma;
+    double tau[3], tau_min;
+    double A[3], B[3], C[3], D[3];
+    double chi_p[3];     // Parabola::chi = 1/(2A)            (:85)
+    double neg_q_A[3];   // -0.25/A of Parabola::psi           (:87)
+    double two_A[3];     // 2.0*A of Parabola::c_at_mu         (:84)
+    double psi_t[3];     // psi_a(mu_ref) - psi_gamma(mu_ref)  (:797)
+    double mu_ref;
+    double dt_max, dt_min, max_phase_change, cg_rtol, cg_atol, closure_tol, energy_rtol, energy_atol;
+    double mass_scale;    // gx*gy*dx*dy*1e-6                  (:1152)
+    double energy_scale;  // sigma*max(gx*dx, gy*dy)            (:1157)
+    int cg_max, max_retries, check_energy, phase_only;
+};
+
+// Device buffers: two state sets (current / trial, selected by Ctl::cur) and
+// the work vectors of the implicit solve.  Every plane is ny rows of `pitch`
+// doubles (pitch = nx rounded up to 32, so each row starts on 256 B).
+struct DevBufs {
+    double* phi[2][3];
+    double* c[2];
+    double* mu[2];
+    double* K;     // transport K = sum phi_p D_p chi_p of trial phi
+    double* chi;   // susceptibility of trial phi
+    double* icpt;  // composition(mu_ref) of trial phi
+    double* diag;  // Jacobi preconditioner
+    double* x;     // mu - mu_ref (the CG unknown)
+    double* r;
+    double* z;
+    double* p[2];  // search direction, double-buffered (read at neighbours while rewritten)
+    double* Ap;
+    double* part;  // [2][grid][kMaxRed] block partials
+    struct Ctl* ctl;
+};
+
+// Device-resident control block: barrier words, the State scalars and the
+// results of the last launch.  Host and device exchange it by value.
+struct Ctl {
+    unsigned bar_count;
+    unsigned pad0[31];
+    unsigned bar_gen;
+    unsigned pad1[31];
+    int status, why, cur, energy_valid;
+    pearl_scalars S;
+    double e0, mass0;
+    pearl_step_info last;
+    long long steps, cg_total;
+    int cg_peak, reached_stop;
+    double out[8];
+    int iout[4];
+};
+
+// ---------------------------------------------------------------- thermodynamics
+// Parabola::psi (pearl_serial.cpp:86-89)
+__device__ __forceinline__ double psi(const DevParams& P, int a, double mu) {
+    const double d = mu - P.B[a];
+    return fma(P.neg_q_A[a], d * d, P.C[a]);
+}
+
+// mixture (pearl_serial.cpp:125-138): returns false where the reference throws.
+__device__ __forceinline__ bool mixture(const DevParams& P, double p0, double p1, double p2, double& chi,
+                                        double& cint, double& K) {
+    const double triple = 2.0 * p0 * p1 * p2;
+    const double h0 = p0 * p0 * (3.0 - 2.0 * p0) + triple;
+    const double h1 = p1 * p1 * (3.0 - 2.0 * p1) + triple;
+    const double h2 = p2 * p2 * (3.0 - 2.0 * p2) + triple;
+    double s = 0.0, ci = 0.0, k = 0.0;
+    s += h0 * P.chi_p[0];
+    ci -= h0 * P.chi_p[0] * P.B[0];
+    k += p0 * P.D[0] * P.chi_p[0];
+    s += h1 * P.chi_p[1];
+    ci -= h1 * P.chi_p[1] * P.B[1];
+    k += p1 * P.D[1] * P.chi_p[1];
+    s += h2 * P.chi_p[2];
+    ci -= h2 * P.chi_p[2] * P.B[2];
+    k += p2 * P.D[2] * P.chi_p[2];
+    chi = s;
+    cint = ci;
+    K = k;
+    return (s > 0.0) && isfinite(s) && isfinite(ci) && isfinite(k) && !(k < 0.0);
+}
+
+// project_simplex (pearl_serial.cpp:491-509).  Inputs are finite here (the
+// caller checks first, :990-996).  Returns false where the reference throws.
+__device__ __forceinline__ bool project_simplex(double& z0, double& z1, double& z2) {
+    double s0 = z0, s1 = z1, s2 = z2, t;
+    if (s0 < s1) { t = s0; s0 = s1; s1 = t; }
+    if (s1 < s2) { t = s1; s1 = s2; s2 = t; }
+    if (s0 < s1) { t = s0; s0 = s1; s1 = t; }
+    double sum = 0.0, threshold = 0.0, cand;
+    int active = 0;
+    sum += s0;
+    cand = (sum - 1.0) / 1;
+    if (s0 > cand) { active = 1; threshold = cand; }
+    sum += s1;
+    cand = (sum - 1.0) / 2;
+    if (s1 > cand) { active = 2; threshold = cand; }
+    sum += s2;
+    cand = (sum - 1.0) / 3;
+    if (s2 > cand) { active = 3; threshold = cand; }
+    // std::max(0.0, v) == (0.0 < v ? v : 0.0)
+    double v = z0 - threshold;
+    z0 = (0.0 < v) ? v : 0.0;
+    v = z1 - threshold;
+    z1 = (0.0 < v) ? v : 0.0;
+    v = z2 - threshold;
+    z2 = (0.0 < v) ? v : 0.0;
+    return active != 0;
+}
+
+// local_tau (pearl_serial.cpp:533-537)
+__device__ __forceinline__ double local_tau(const DevParams& P, double p0, double p1, double p2) {
+    const double w0 = p0 * p1, w1 = p0 * p2, w2 = p1 * p2;
+    const double s = w0 + w1 + w2;
+    return s > 1e-30 ? (w0 * P.tau[0] + w1 * P.tau[1] + w2 * P.tau[2]) / s : P.tau_min;
+}
+
+// ---------------------------------------------------------------- grid barrier
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;  // 4 s; a phase takes well under 0.1 s
+
+// Sense-by-generation grid barrier for a cooperative launch (all blocks are
+// co-resident).  The wait is bounded: after kBarrierTimeoutNs the block
+// records PEARL_ERR_DEVICE_WAIT and every caller returns without further
+// device work.  Memory ordering follows the cooperative-groups pattern:
+// block barrier, fence, arrive, wait, fence, block barrier.
+__device__ __forceinline__ bool grid_barrier(Ctl* ctl, unsigned nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned* vgen = &ctl->bar_gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->bar_count, 1u);
+        if (prev == nblocks - 1) {
+            atomicExch(&ctl->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&ctl->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (*vgen == g) {
+                if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                    ok = 0;
+                    atomicCAS(&ctl->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// ---------------------------------------------------------------- reductions
+// Deterministic reductions: fixed shuffle trees inside a warp, warps combined
+// in index order, blocks combined in index order by every block identically,
+// so all blocks hold bitwise-equal results and take the same decisions.
+enum RedOp : unsigned { kSum = 0, kMax = 1, kMin = 2 };
+
+__device__ __forceinline__ double red_apply(unsigned op, double a, double b) {
+    // fmax/fmin drop NaN like the reference's std::max(acc, v)/std::min(acc, v)
+    return op == kSum ? a + b : (op == kMax ? fmax(a, b) : fmin(a, b));
+}
+__device__ __forceinline__ double red_identity(unsigned op) {
+    return op == kSum ? 0.0 : (op == kMax ? -INFINITY : INFINITY);
+}
+__device__ __forceinline__ unsigned op_of(unsigned ops, int k) { return (ops >> (2 * k)) & 3u; }
+
+template <int NV>
+__device__ __forceinline__ void block_publish(const double (&v)[NV], unsigned ops, double* part_slot) {
+    __shared__ double s_red[kThreads / 32][kMaxRed];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        const unsigned op = op_of(ops, k);
+        double t = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t = red_apply(op, t, __shfl_down_sync(0xffffffffu, t, o));
+        if (lane == 0) s_red[warp][k] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const unsigned op = op_of(ops, k);
+            double acc = s_red[0][k];
+            for (int w = 1; w < kThreads / 32; ++w) acc = red_apply(op, acc, s_red[w][k]);
+            part_slot[blockIdx.x * kMaxRed + k] = acc;
+        }
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void grid_gather(double (&out)[NV], unsigned ops, const double* part_slot) {
+    __shared__ double s_out[kMaxRed];
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const unsigned op = op_of(ops, k);
+            double acc = red_identity(op);
+            for (int b = lane; b < (int)gridDim.x; b += 32) acc = red_apply(op, acc, part_slot[b * kMaxRed + k]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc = red_apply(op, acc, __shfl_down_sync(0xffffffffu, acc, o));
+            if (lane == 0) s_out[k] = acc;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = s_out[k];
+    __syncthreads();
+}
+
+}  // namespace pearl_gpu

@@ -1,0 +1,1445 @@
+// pearl_fp64.cu — FP64 hot path of Pearl on B200: one persistent cooperative
+// kernel runs whole accepted time steps (pearl::advance, pearl_serial.cpp:1119)
+// including the retry loop and the Jacobi-PCG solve, with every decision
+// (dt, acceptance, CG termination) taken on the device.
+//
+// Phases of one attempt (each is a sweep over 32x8-cell tiles followed by a
+// deterministic grid reduction and a bounded grid barrier):
+//   PROPOSE  propose_phi (:961-1002) + mixture of the trial phi (:1013-1020)
+//   SETUP    implicit_diffusion set-up: apply(mu_offset), r, z, diag (:1021-1046)
+//   APPLY    p = z + beta p ; A p ; <p,Ap>                          (:1067-1079)
+//   UPDATE   x += alpha p ; r -= alpha Ap ; z = r/diag ; <r,z>,<r,r> (:1071-1078)
+//   TRUE_RES r = rhs - A x ; <r,r>                                   (:1051-1055)
+//   RESET    z = r/diag ; <r,z>                                      (:1060-1064)
+//   FINAL    conservative carbon update, closure, mu, valid_state,
+//            total_carbon and reduced_energy of the trial state      (:1082-1093, :1096-1116, :784-821)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pearl_device.cuh"
+#include "pearl_gpu.h"
+
+namespace pearl_gpu {
+
+enum Mode : int {
+    kModeRun = 0,
+    kModePropose = 1,
+    kModeMix = 2,
+    kModeDiffusion = 3,
+    kModeEnergy = 4,
+    kModeValid = 5,
+    kModeSnapshot = 6,
+    kModeMaybeShift = 7,
+};
+
+struct KArgs {
+    DevParams P;
+    DevBufs B;
+    int mode;
+    double dt;  // diagnostic modes
+    pearl_run_limits L;
+    double shift_trigger, shift_target, shift_c_gamma;
+};
+
+struct Cell {
+    int x, y;
+    size_t i, iw, ie, is, in;
+    bool ok;
+};
+
+__device__ __forceinline__ Cell cell_of(const DevParams& P, int t) {
+    Cell c;
+    const int bx = t % P.ntx, by = t / P.ntx;
+    c.x = bx * kTileX + (threadIdx.x & 31);
+    c.y = by * kTileY + (threadIdx.x >> 5);
+    c.ok = c.x < P.nx && c.y < P.ny;
+    const int xw = c.x == 0 ? P.nx - 1 : c.x - 1;
+    const int xe = c.x == P.nx - 1 ? 0 : c.x + 1;
+    const size_t row = (size_t)c.y * P.pitch;
+    c.i = row + c.x;
+    c.iw = row + xw;
+    c.ie = row + xe;
+    // zero-flux ghosts copy the edge row (pearl_serial.cpp:690-691)
+    c.is = c.y > 0 ? c.i - P.pitch : c.i;
+    c.in = c.y < P.ny - 1 ? c.i + P.pitch : c.i;
+    return c;
+}
+
+// Face weights of implicit_diffusion's weights_at (pearl_serial.cpp:1022-1028)
+struct Faces {
+    double w0, w1, w2, w3;
+};
+__device__ __forceinline__ Faces faces_at(const DevParams& P, const double* K, const Cell& c) {
+    const double k = K[c.i];
+    Faces f;
+    f.w0 = .5 * (k + K[c.iw]) / P.dx2;
+    f.w1 = .5 * (k + K[c.ie]) / P.dx2;
+    f.w2 = .5 * (k + K[c.is]) / P.dy2;
+    f.w3 = .5 * (k + K[c.in]) / P.dy2;
+    if (c.y == 0) f.w2 = 0;
+    if (c.y == P.ny - 1) f.w3 = 0;
+    return f;
+}
+
+// apply (pearl_serial.cpp:1029-1035): chi*u + dt*sum_f w_f (u - u_f)
+__device__ __forceinline__ double apply_at(double chi, double dt, const Faces& f, double u, double uw, double ue,
+                                           double us, double un) {
+    return chi * u + dt * (f.w0 * (u - uw) + f.w1 * (u - ue) + f.w2 * (u - us) + f.w3 * (u - un));
+}
+
+// Per-cell reduced-energy density of reduced_energy (pearl_serial.cpp:800-819),
+// without the final dx*dy.  chi/icpt are mixture(phi).susceptibility and
+// composition(mu_ref, mixture(phi)).
+__device__ __forceinline__ double energy_cell(const DevParams& P, const Cell& c, double q0, double q1, double q2,
+                                              const double* const* phi, double carbon, double chi, double icpt) {
+    const double triple = 2.0 * q0 * q1 * q2;
+    const double h0 = q0 * q0 * (3.0 - 2.0 * q0) + triple;
+    const double h1 = q1 * q1 * (3.0 - 2.0 * q1) + triple;
+    const double h2 = q2 * q2 * (3.0 - 2.0 * q2) + triple;
+    double chem = 0;
+    chem += h0 * P.psi_t[0];
+    chem += h1 * P.psi_t[1];
+    chem += h2 * P.psi_t[2];
+    if (!P.phase_only) {
+        const double dc = carbon - icpt;
+        chem += .5 * dc * dc / chi;
+    }
+    double t = chem / P.Vm + P.obs * (q0 * q1 + q0 * q2 + q1 * q2) + P.tr * q0 * q1 * q2;
+    {
+        const double n0 = phi[0][c.ie], n1 = phi[1][c.ie], n2 = phi[2][c.ie];
+        double z = (q0 * n1 - n0 * q1) / P.dx;
+        t += P.eps_sigma * z * z;
+        z = (q0 * n2 - n0 * q2) / P.dx;
+        t += P.eps_sigma * z * z;
+        z = (q1 * n2 - n1 * q2) / P.dx;
+        t += P.eps_sigma * z * z;
+    }
+    if (c.y != P.ny - 1) {
+        const double n0 = phi[0][c.in], n1 = phi[1][c.in], n2 = phi[2][c.in];
+        double z = (q0 * n1 - n0 * q1) / P.dy;
+        t += P.eps_sigma * z * z;
+        z = (q0 * n2 - n0 * q2) / P.dy;
+        t += P.eps_sigma * z * z;
+        z = (q1 * n2 - n1 * q2) / P.dy;
+        t += P.eps_sigma * z * z;
+    }
+    return t;
+}
+
+// valid_state per cell (pearl_serial.cpp:1099-1114); true if the cell is bad.
+__device__ __forceinline__ bool bad_cell(const DevParams& P, double q0, double q1, double q2, double carbon,
+                                         double mu) {
+    bool good = true;
+    double sum = 0;
+    good = good && isfinite(q0) && q0 >= -1e-12 && q0 <= 1 + 1e-12;
+    sum += q0;
+    good = good && isfinite(q1) && q1 >= -1e-12 && q1 <= 1 + 1e-12;
+    sum += q1;
+    good = good && isfinite(q2) && q2 >= -1e-12 && q2 <= 1 + 1e-12;
+    sum += q2;
+    good = good && fabs(sum - 1) < 1e-10;
+    good = good && isfinite(mu) && isfinite(carbon);
+    if (!P.phase_only) {
+        good = good && carbon >= -1e-10 && carbon <= 1 + 1e-10;
+        const double q[3] = {q0, q1, q2};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (q[a] > .01) {
+                const double ca = (mu - P.B[a]) / P.two_A[a];
+                good = good && ca >= -1e-10 && ca <= 1 + 1e-10;
+            }
+    }
+    return !good;
+}
+
+// ------------------------------------------------------------------ the kernel
+struct Red {
+    const KArgs& a;
+    unsigned counter = 0;
+    __device__ explicit Red(const KArgs& args) : a(args) {}
+    // publish the block partials, wait for the grid, combine; false on a device-wait timeout
+    template <int NV>
+    __device__ bool reduce(double (&v)[NV], unsigned ops) {
+        double* slot = a.B.part + (size_t)(counter & 1u) * gridDim.x * kMaxRed;
+        ++counter;
+        block_publish<NV>(v, ops, slot);
+        if (!grid_barrier(a.B.ctl, gridDim.x)) return false;
+        grid_gather<NV>(v, ops, slot);
+        return true;
+    }
+};
+
+#define OPS2(a, b) ((unsigned)(a) | ((unsigned)(b) << 2))
+#define OPS3(a, b, c) (OPS2(a, b) | ((unsigned)(c) << 4))
+#define OPS4(a, b, c, d) (OPS3(a, b, c) | ((unsigned)(d) << 6))
+#define OPS5(a, b, c, d, e) (OPS4(a, b, c, d) | ((unsigned)(e) << 8))
+
+// PROPOSE: propose_phi from state `cur` into state `1-cur`, then the mixture of
+// the trial phi (K, chi, icpt); in phase_only mode also the reconstructed
+// trial carbon and the copied trial mu (pearl_serial.cpp:1134-1136).
+// Reduction: {max |dphi| (inf if non-finite), mixture invalid, simplex failed}.
+__device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, double& change, bool& mixbad,
+                              bool& simplexbad) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[cur];
+    double* const* tp = B.phi[cur ^ 1];
+    double vchange = 0, vmix = 0, vsimp = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const double q0 = ph[0][c.i], q1 = ph[1][c.i], q2 = ph[2][c.i];
+        const double mu = B.mu[cur][c.i];
+        const double psi0 = psi(P, 2, mu);
+        const double ps[3] = {psi(P, 0, mu), psi(P, 1, mu), psi0};
+        const double q[3] = {q0, q1, q2};
+        const double dtr[3] = {2.0 * q1 * q2, 2.0 * q0 * q2, 2.0 * q0 * q1};
+        double f[3];
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa) {
+            const double qa1 = q[(aa + 1) % 3], qa2 = q[(aa + 2) % 3];
+            f[aa] = P.obs * (qa1 + qa2) + P.tr * qa1 * qa2;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const double dh = dtr[aa] + (b == aa ? 6.0 * q[b] * (1.0 - q[b]) : 0.0);
+                f[aa] += (ps[b] - psi0) * dh / P.Vm;
+            }
+        }
+        // four faces in the reference's order: -x, +x, -y (not at y=0), +y (not at top)
+#pragma unroll
+        for (int dir = 0; dir < 4; ++dir) {
+            if ((dir == 2 && c.y == 0) || (dir == 3 && c.y == P.ny - 1)) continue;
+            const size_t j = dir == 0 ? c.iw : (dir == 1 ? c.ie : (dir == 2 ? c.is : c.in));
+            const double n[3] = {ph[0][j], ph[1][j], ph[2][j]};
+            const double d2 = dir < 2 ? P.dx2 : P.dy2;
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                for (int b = aa + 1; b < 3; ++b) {
+                    const double w = P.two_eps_sigma * (q[aa] * n[b] - n[aa] * q[b]) / d2;
+                    f[aa] += w * n[b];
+                    f[b] -= w * n[aa];
+                }
+        }
+        const double mean = (f[0] + f[1] + f[2]) / 3, scale = dt / (local_tau(P, q0, q1, q2) * P.eps);
+        double z0 = q0 - scale * (f[0] - mean), z1 = q1 - scale * (f[1] - mean), z2 = q2 - scale * (f[2] - mean);
+        if (!(isfinite(z0) && isfinite(z1) && isfinite(z2))) {
+            vchange = INFINITY;
+            z0 = q0;
+            z1 = q1;
+            z2 = q2;
+        } else {
+            if (!project_simplex(z0, z1, z2)) vsimp = 1;
+            vchange = fmax(vchange, fabs(z0 - q0));
+            vchange = fmax(vchange, fabs(z1 - q1));
+            vchange = fmax(vchange, fabs(z2 - q2));
+        }
+        tp[0][c.i] = z0;
+        tp[1][c.i] = z1;
+        tp[2][c.i] = z2;
+        double chi, cint, K;
+        if (!mixture(P, z0, z1, z2, chi, cint, K)) vmix = 1;
+        B.K[c.i] = K;
+        B.chi[c.i] = chi;
+        B.icpt[c.i] = fma(chi, P.mu_ref, cint);
+        if (P.phase_only) {
+            B.c[cur ^ 1][c.i] = fma(chi, mu, cint);
+            B.mu[cur ^ 1][c.i] = mu;
+        }
+    }
+    double v[3] = {vchange, vmix, vsimp};
+    if (!red.reduce<3>(v, OPS3(kMax, kMax, kMax))) return false;
+    change = v[0];
+    mixbad = v[1] != 0;
+    simplexbad = v[2] != 0;
+    return true;
+}
+
+// MIX: K, chi, icpt of the trial phi (used when the trial phi was uploaded).
+__device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    double* const* tp = B.phi[cur ^ 1];
+    double vmix = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        double chi, cint, K;
+        if (!mixture(P, tp[0][c.i], tp[1][c.i], tp[2][c.i], chi, cint, K)) vmix = 1;
+        B.K[c.i] = K;
+        B.chi[c.i] = chi;
+        B.icpt[c.i] = fma(chi, P.mu_ref, cint);
+    }
+    double v[1] = {vmix};
+    if (!red.reduce<1>(v, kMax)) return false;
+    mixbad = v[0] != 0;
+    return true;
+}
+
+// SETUP: apply(mu_offset) and the initial residual (pearl_serial.cpp:1036-1046).
+// Reduction: {<rhs,rhs>, <r,z>, <r,r>}.
+__device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double& rhs2, double& rz, double& rr) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* mu = B.mu[cur];
+    const double* cold = B.c[cur];
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const Faces f = faces_at(P, B.K, c);
+        const double chi = B.chi[c.i];
+        const double u = mu[c.i] - P.mu_ref;
+        const double Au = apply_at(chi, dt, f, u, mu[c.iw] - P.mu_ref, mu[c.ie] - P.mu_ref, mu[c.is] - P.mu_ref,
+                                   mu[c.in] - P.mu_ref);
+        const double diag = chi + dt * (f.w0 + f.w1 + f.w2 + f.w3);
+        const double rhs = cold[c.i] - B.icpt[c.i];
+        const double r = rhs - Au;
+        const double z = r / diag;
+        B.x[c.i] = u;
+        B.r[c.i] = r;
+        B.z[c.i] = z;
+        B.diag[c.i] = diag;
+        s0 += rhs * rhs;
+        s1 += r * z;
+        s2 += r * r;
+    }
+    double v[3] = {s0, s1, s2};
+    if (!red.reduce<3>(v, OPS3(kSum, kSum, kSum))) return false;
+    rhs2 = v[0];
+    rz = v[1];
+    rr = v[2];
+    return true;
+}
+
+// APPLY: p_new = z (first) or z + beta*p_old, written to p[pout]; Ap; <p,Ap>.
+__device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* z = B.z;
+    const double* po = B.p[pout ^ 1];
+    double* pn = B.p[pout];
+    double s = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const Faces f = faces_at(P, B.K, c);
+        double pc, pw, pe, ps, pnn;
+        if (first) {
+            pc = z[c.i];
+            pw = z[c.iw];
+            pe = z[c.ie];
+            ps = z[c.is];
+            pnn = z[c.in];
+        } else {
+            pc = z[c.i] + beta * po[c.i];
+            pw = z[c.iw] + beta * po[c.iw];
+            pe = z[c.ie] + beta * po[c.ie];
+            ps = z[c.is] + beta * po[c.is];
+            pnn = z[c.in] + beta * po[c.in];
+        }
+        const double Ap = apply_at(B.chi[c.i], dt, f, pc, pw, pe, ps, pnn);
+        pn[c.i] = pc;
+        B.Ap[c.i] = Ap;
+        s += pc * Ap;
+    }
+    double v[1] = {s};
+    if (!red.reduce<1>(v, kSum)) return false;
+    pAp = v[0];
+    return true;
+}
+
+// UPDATE: x += alpha p; r -= alpha Ap; z = r/diag; {<r,z>, <r,r>}.
+__device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* p = B.p[pcur];
+    double s0 = 0, s1 = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const double x = B.x[c.i] + alpha * p[c.i];
+        const double r = B.r[c.i] - alpha * B.Ap[c.i];
+        const double z = r / B.diag[c.i];
+        B.x[c.i] = x;
+        B.r[c.i] = r;
+        B.z[c.i] = z;
+        s0 += r * z;
+        s1 += r * r;
+    }
+    double v[2] = {s0, s1};
+    if (!red.reduce<2>(v, OPS2(kSum, kSum))) return false;
+    rz = v[0];
+    rr = v[1];
+    return true;
+}
+
+// TRUE_RES: r = rhs - A x; <r,r>  (pearl_serial.cpp:1051-1055)
+__device__ bool phase_true_residual(const KArgs& a, Red& red, int cur, double dt, double& rr) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* x = B.x;
+    double s = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const Faces f = faces_at(P, B.K, c);
+        const double Ax = apply_at(B.chi[c.i], dt, f, x[c.i], x[c.iw], x[c.ie], x[c.is], x[c.in]);
+        const double r = (B.c[cur][c.i] - B.icpt[c.i]) - Ax;
+        B.r[c.i] = r;
+        s += r * r;
+    }
+    double v[1] = {s};
+    if (!red.reduce<1>(v, kSum)) return false;
+    rr = v[0];
+    return true;
+}
+
+// RESET: z = r/diag; <r,z>  (pearl_serial.cpp:1060-1064)
+__device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    double s = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const double r = B.r[c.i];
+        const double z = r / B.diag[c.i];
+        B.z[c.i] = z;
+        s += r * z;
+    }
+    double v[1] = {s};
+    if (!red.reduce<1>(v, kSum)) return false;
+    rz = v[0];
+    return true;
+}
+
+// FINAL: carbon update, closure and mu (pearl_serial.cpp:1082-1093) fused with
+// valid_state, total_carbon and reduced_energy of the trial state.
+// Reduction: {closure max, bad max, carbon sum, energy sum}.
+__device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double& closure, bool& bad,
+                            double& mass, double& energy) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const int tr = cur ^ 1;
+    const double* x = B.x;
+    const double* const* tp = B.phi[tr];
+    double vclos = 0, vbad = 0, vmass = 0, ven = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const Faces f = faces_at(P, B.K, c);
+        const double u = x[c.i];
+        const double change =
+            dt * (f.w0 * (x[c.iw] - u) + f.w1 * (x[c.ie] - u) + f.w2 * (x[c.is] - u) + f.w3 * (x[c.in] - u));
+        const double chi = B.chi[c.i], icpt = B.icpt[c.i];
+        const double cn = B.c[cur][c.i] + change;
+        vclos = fmax(vclos, fabs(cn - (icpt + chi * u)));
+        const double mun = P.mu_ref + (cn - icpt) / chi;
+        B.c[tr][c.i] = cn;
+        B.mu[tr][c.i] = mun;
+        const double q0 = tp[0][c.i], q1 = tp[1][c.i], q2 = tp[2][c.i];
+        if (bad_cell(P, q0, q1, q2, cn, mun)) vbad = 1;
+        vmass += cn;
+        ven += energy_cell(P, c, q0, q1, q2, tp, cn, chi, icpt);
+    }
+    double v[4] = {vclos, vbad, vmass, ven};
+    if (!red.reduce<4>(v, OPS4(kMax, kMax, kSum, kSum))) return false;
+    closure = v[0];
+    bad = v[1] != 0;
+    mass = v[2] * P.dx * P.dy;
+    energy = v[3] * P.dx * P.dy;
+    return true;
+}
+
+// PHASE_ONLY FINAL: valid_state and reduced_energy of the trial state whose
+// carbon and mu were written by PROPOSE.  Reduction: {bad max, energy sum}.
+__device__ bool phase_final_phase_only(const KArgs& a, Red& red, int cur, bool& bad, double& energy) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const int tr = cur ^ 1;
+    const double* const* tp = B.phi[tr];
+    double vbad = 0, ven = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const double q0 = tp[0][c.i], q1 = tp[1][c.i], q2 = tp[2][c.i];
+        if (bad_cell(P, q0, q1, q2, B.c[tr][c.i], B.mu[tr][c.i])) vbad = 1;
+        ven += energy_cell(P, c, q0, q1, q2, tp, 0.0, B.chi[c.i], B.icpt[c.i]);
+    }
+    double v[2] = {vbad, ven};
+    if (!red.reduce<2>(v, OPS2(kMax, kSum))) return false;
+    bad = v[0] != 0;
+    energy = v[1] * P.dx * P.dy;
+    return true;
+}
+
+// ENERGY: reduced_energy and total_carbon of state `s` (the e0, mass0 of
+// advance, pearl_serial.cpp:1122-1123), plus mixture validity and
+// valid_state.  Reduction: {energy sum, carbon sum, mixture invalid, bad}.
+__device__ bool phase_energy(const KArgs& a, Red& red, int s, double& energy, double& mass, bool& mixbad,
+                             bool& bad) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[s];
+    double ven = 0, vmass = 0, vmix = 0, vbad = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const double q0 = ph[0][c.i], q1 = ph[1][c.i], q2 = ph[2][c.i];
+        double chi = 1, cint = 0, K;
+        if (!P.phase_only) {
+            if (!mixture(P, q0, q1, q2, chi, cint, K)) vmix = 1;
+        }
+        const double cc = B.c[s][c.i];
+        ven += energy_cell(P, c, q0, q1, q2, ph, cc, chi, fma(chi, P.mu_ref, cint));
+        vmass += cc;
+        if (bad_cell(P, q0, q1, q2, cc, B.mu[s][c.i])) vbad = 1;
+    }
+    double v[4] = {ven, vmass, vmix, vbad};
+    if (!red.reduce<4>(v, OPS4(kSum, kSum, kMax, kMax))) return false;
+    energy = v[0] * P.dx * P.dy;
+    mass = v[1] * P.dx * P.dy;
+    mixbad = v[2] != 0;
+    bad = v[3] != 0;
+    return true;
+}
+
+__device__ __forceinline__ void set_error(Ctl* ctl, int status, int why) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (atomicCAS(&ctl->status, 0, status) == 0) ctl->why = why;
+    }
+}
+
+// Implicit diffusion: SETUP, Jacobi-PCG (pearl_serial.cpp:1047-1080) and FINAL.
+// Returns false only on a device-wait timeout.  Sets ok/it/residual and, when
+// the solve converged, the FINAL reductions.
+struct DiffusionOut {
+    bool ok;
+    int it;
+    double residual, closure, mass, energy;
+    bool bad;
+};
+
+__device__ bool diffusion(const KArgs& a, Red& red, int cur, double dt, DiffusionOut& o) {
+    const DevParams& P = a.P;
+    o.ok = false;
+    o.it = 0;
+    o.residual = 0;
+    o.closure = 0;
+    o.bad = false;
+    o.mass = 0;
+    o.energy = 0;
+    double rhs2, rz, rr;
+    if (!phase_setup(a, red, cur, dt, rhs2, rz, rr)) return false;
+    const double tolerance = P.cg_atol + P.cg_rtol * sqrt(rhs2);
+    bool first = true;
+    double beta = 0;
+    int pbuf = 0;  // p[pbuf] holds the current search direction
+    for (int iteration = 0; iteration <= P.cg_max; ++iteration) {
+        o.it = iteration;
+        o.residual = sqrt(rr);
+        if (!isfinite(o.residual)) return true;
+        if (o.residual <= tolerance) {
+            if (!phase_true_residual(a, red, cur, dt, rr)) return false;
+            o.residual = sqrt(rr);
+            if (o.residual <= tolerance * 1.05) {
+                o.ok = true;
+                break;
+            }
+            if (!phase_reset(a, red, rz)) return false;
+            first = true;
+            continue;
+        }
+        if (iteration == P.cg_max) break;
+        const int pout = pbuf ^ 1;
+        double pAp;
+        if (!phase_apply(a, red, dt, first, beta, pout, pAp)) return false;
+        pbuf = pout;
+        if (!(pAp > 0) || !isfinite(pAp) || !isfinite(rz)) return true;
+        const double alpha = rz / pAp;
+        double rz_next;
+        if (!phase_update(a, red, alpha, pbuf, rz_next, rr)) return false;
+        beta = rz_next / rz;
+        rz = rz_next;
+        first = false;
+    }
+    if (!o.ok) return true;
+    if (!phase_final(a, red, cur, dt, o.closure, o.bad, o.mass, o.energy)) return false;
+    o.ok = o.closure <= P.closure_tol;
+    return true;
+}
+
+// One pearl::advance (pearl_serial.cpp:1119-1174) on the device.  All blocks
+// execute it with identical scalars.  Returns false when the step ended with
+// an error status (recorded in ctl) or a device-wait timeout.
+struct StepState {
+    pearl_scalars S;
+    int cur;
+    bool cache_valid;
+    double e0, mass0;
+};
+
+__device__ bool advance(const KArgs& a, Red& red, StepState& st, double stop_time, pearl_step_info& info) {
+    const DevParams& P = a.P;
+    Ctl* ctl = a.B.ctl;
+    double dt = st.S.dt;
+    if (P.dt_max < dt) dt = P.dt_max;
+    if (stop_time - st.S.time < dt) dt = stop_time - st.S.time;
+    if (!(dt > 0) || !isfinite(dt)) {
+        set_error(ctl, PEARL_ERR_INVALID_ADVANCE_TIME, 0);
+        return false;
+    }
+    if (!st.cache_valid) {
+        double e, m;
+        bool mixbad, bad;
+        if (!phase_energy(a, red, st.cur, e, m, mixbad, bad)) return false;
+        if (mixbad) {
+            set_error(ctl, PEARL_ERR_MIXTURE, 0);
+            return false;
+        }
+        st.e0 = P.check_energy ? e : 0;
+        st.mass0 = P.phase_only ? 0 : m;
+        st.cache_valid = true;
+    }
+    int why = PEARL_WHY_NONE;
+    for (int attempt = 0; attempt <= P.max_retries; ++attempt) {
+        pearl_step_info out;
+        memset(&out, 0, sizeof out);
+        out.retries = attempt;
+        out.accepted_dt = dt;
+        bool mixbad, simplexbad;
+        if (!phase_propose(a, red, st.cur, dt, out.max_phase_change, mixbad, simplexbad)) return false;
+        if (simplexbad) {
+            set_error(ctl, PEARL_ERR_SIMPLEX, 0);
+            return false;
+        }
+        bool good = isfinite(out.max_phase_change) && out.max_phase_change <= P.max_phase_change;
+        why = PEARL_WHY_PHASE_INCREMENT;
+        bool bad = false;
+        double mass = 0, e1 = 0;
+        if (good) {
+            if (mixbad) {
+                set_error(ctl, PEARL_ERR_MIXTURE, 0);
+                return false;
+            }
+            if (P.phase_only) {
+                if (!phase_final_phase_only(a, red, st.cur, bad, e1)) return false;
+            } else {
+                DiffusionOut d;
+                if (!diffusion(a, red, st.cur, dt, d)) return false;
+                good = d.ok;
+                out.cg_iterations = d.it;
+                out.linear_residual = d.residual;
+                out.closure = d.closure;
+                why = PEARL_WHY_LINEAR_CLOSURE;
+                bad = d.bad;
+                mass = d.mass;
+                e1 = d.energy;
+            }
+        }
+        if (good) {
+            good = !bad;
+            why = PEARL_WHY_BOUNDS;
+        }
+        if (good && !P.phase_only) {
+            good = fabs(mass - st.mass0) <= 1e-11 * fmax(fabs(st.mass0), P.mass_scale);
+            why = PEARL_WHY_MASS;
+        }
+        if (good && P.check_energy) {
+            out.energy_change = e1 - st.e0;
+            const double tol = P.energy_atol + P.energy_rtol * fmax(fabs(st.e0), P.energy_scale);
+            good = isfinite(e1) && e1 <= st.e0 + tol;
+            why = PEARL_WHY_ENERGY;
+        }
+        if (good) {
+            st.S.time = st.S.time + dt;
+            st.S.step = st.S.step + 1;
+            st.S.rejected = st.S.rejected + attempt;
+            const double grown = dt * 1.1;
+            st.S.dt = grown < P.dt_max ? grown : P.dt_max;
+            st.cur ^= 1;
+            st.e0 = P.check_energy ? e1 : 0;
+            st.mass0 = P.phase_only ? 0 : mass;
+            info = out;
+            return true;
+        }
+        dt *= .5;
+        if (dt < P.dt_min) {
+            set_error(ctl, PEARL_ERR_REJECTED_BELOW_DT_MIN, why);
+            return false;
+        }
+    }
+    set_error(ctl, PEARL_ERR_RETRY_LIMIT, why);
+    return false;
+}
+
+// Moving window on the device (maybe_shift + shift_rows, pearl_serial.cpp:2023-2071).
+__device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_out) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    rows_out = 0;
+    const int cur = st.cur;
+    const double* g = B.phi[cur][2];
+    double local = -1;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok || c.y == P.ny - 1) continue;
+        const double av = 1 - 2 * g[c.i], bv = 1 - 2 * g[c.in];
+        if (av >= 0 && bv < 0) local = fmax(local, ((c.y + 1) - .5 + av / (av - bv)) * P.dy);
+    }
+    double v1[1] = {local};
+    if (!red.reduce<1>(v1, kMax)) return false;
+    const double front = v1[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.B.ctl->out[0] = front;
+    if (front < a.shift_trigger) return true;
+    const int rows = (int)floor((front - a.shift_target) / P.dy);
+    double gmax = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok || c.y >= rows) continue;
+        gmax = fmax(gmax, g[c.i]);
+    }
+    double v2[1] = {gmax};
+    if (!red.reduce<1>(v2, kMax)) return false;
+    if (v2[0] > 1e-6) {
+        set_error(B.ctl, PEARL_ERR_UNSAFE_SHIFT, 0);
+        return false;
+    }
+    if (rows <= 0 || rows >= P.ny || a.shift_c_gamma < 0 || a.shift_c_gamma > 1) {
+        set_error(B.ctl, PEARL_ERR_INVALID_ARGUMENT, 0);
+        return false;
+    }
+    const int nw = cur ^ 1;
+    double removed = 0, vmix = 0, vnonfin = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        if (c.y < rows) removed += B.c[cur][c.i] * P.dx * P.dy;
+        double q0, q1, q2, cc;
+        if (c.y + rows < P.ny) {
+            const size_t j = c.i + (size_t)rows * P.pitch;
+            q0 = B.phi[cur][0][j];
+            q1 = B.phi[cur][1][j];
+            q2 = B.phi[cur][2][j];
+            cc = B.c[cur][j];
+        } else {
+            q0 = 0;
+            q1 = 0;
+            q2 = 1;
+            cc = a.shift_c_gamma;
+        }
+        B.phi[nw][0][c.i] = q0;
+        B.phi[nw][1][c.i] = q1;
+        B.phi[nw][2][c.i] = q2;
+        B.c[nw][c.i] = cc;
+        double chi, cint, K;
+        if (!mixture(P, q0, q1, q2, chi, cint, K)) vmix = 1;
+        if (!isfinite(cc)) vnonfin = 1;
+        B.mu[nw][c.i] = (cc - cint) / chi;  // close_mu / reconstruct_mu (:139-142, :789-792)
+    }
+    double v3[3] = {removed, vmix, vnonfin};
+    if (!red.reduce<3>(v3, OPS3(kSum, kMax, kMax))) return false;
+    if (v3[1] != 0) {
+        set_error(B.ctl, PEARL_ERR_MIXTURE, 0);
+        return false;
+    }
+    if (v3[2] != 0) {
+        set_error(B.ctl, PEARL_ERR_NONFINITE_CARBON, 0);
+        return false;
+    }
+    const double added = rows * P.nx * a.shift_c_gamma * P.dx * P.dy;
+    st.S.shift_distance += rows * P.dy;
+    st.S.shifts++;
+    st.S.carbon_added += added;
+    st.S.carbon_removed += v3[0];
+    st.cur = nw;
+    st.cache_valid = false;
+    rows_out = rows;
+    return true;
+}
+
+// snapshot() reductions (pearl_serial.cpp:2266-2281) on state `s`.
+__device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[s];
+    double minc = 1e300, maxc = -1e300, minmu = 1e300, maxmu = -1e300, sumerr = 0;
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
+        const Cell c = cell_of(P, t);
+        if (!c.ok) continue;
+        const double cc = B.c[s][c.i], mu = B.mu[s][c.i];
+        minc = fmin(minc, cc);
+        maxc = fmax(maxc, cc);
+        minmu = fmin(minmu, mu);
+        maxmu = fmax(maxmu, mu);
+        sumerr = fmax(sumerr, fabs(ph[0][c.i] + ph[1][c.i] + ph[2][c.i] - 1));
+    }
+    double v[5] = {minc, maxc, minmu, maxmu, sumerr};
+    if (!red.reduce<5>(v, OPS5(kMin, kMax, kMin, kMax, kMax))) return false;
+    for (int k = 0; k < 5; ++k) out[k] = v[k];
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs a) {
+    Ctl* ctl = a.B.ctl;
+    Red red(a);
+    StepState st;
+    st.S = ctl->S;
+    st.cur = ctl->cur;
+    st.cache_valid = ctl->energy_valid != 0;
+    st.e0 = ctl->e0;
+    st.mass0 = ctl->mass0;
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+
+    if (a.mode == kModeRun) {
+        long long steps = 0, cg_total = 0;
+        int cg_peak = 0, reached = 0;
+        pearl_step_info last;
+        memset(&last, 0, sizeof last);
+        while (steps < a.L.max_steps) {
+            if (!(st.S.time < a.L.end_time)) break;
+            if (st.S.step >= a.L.config_max_steps) {
+                set_error(ctl, PEARL_ERR_MAX_STEPS, 0);
+                break;
+            }
+            pearl_step_info info;
+            if (!advance(a, red, st, a.L.stop_time, info)) break;
+            ++steps;
+            cg_total += info.cg_iterations;
+            cg_peak = info.cg_iterations > cg_peak ? info.cg_iterations : cg_peak;
+            last = info;
+            if (st.S.time >= a.L.stop_time - a.L.output_eps) {
+                reached = 1;
+                break;
+            }
+        }
+        if (leader) {
+            ctl->S = st.S;
+            ctl->cur = st.cur;
+            ctl->energy_valid = st.cache_valid ? 1 : 0;
+            ctl->e0 = st.e0;
+            ctl->mass0 = st.mass0;
+            ctl->steps = steps;
+            ctl->cg_total = cg_total;
+            ctl->cg_peak = cg_peak;
+            ctl->reached_stop = reached;
+            ctl->last = last;
+        }
+        return;
+    }
+    if (a.mode == kModePropose) {
+        double change;
+        bool mixbad, simplexbad;
+        if (!phase_propose(a, red, st.cur, a.dt, change, mixbad, simplexbad)) return;
+        if (leader) {
+            ctl->out[0] = change;
+            ctl->iout[0] = mixbad;
+            ctl->iout[1] = simplexbad;
+        }
+        return;
+    }
+    if (a.mode == kModeMix) {
+        bool mixbad;
+        if (!phase_mix(a, red, st.cur, mixbad)) return;
+        if (leader) ctl->iout[0] = mixbad;
+        return;
+    }
+    if (a.mode == kModeDiffusion) {
+        DiffusionOut d;
+        if (!diffusion(a, red, st.cur, a.dt, d)) return;
+        if (leader) {
+            ctl->iout[0] = d.ok;
+            ctl->iout[1] = d.it;
+            ctl->out[0] = d.residual;
+            ctl->out[1] = d.closure;
+        }
+        return;
+    }
+    if (a.mode == kModeEnergy || a.mode == kModeValid) {
+        double e, m;
+        bool mixbad, bad;
+        if (!phase_energy(a, red, st.cur, e, m, mixbad, bad)) return;
+        if (leader) {
+            ctl->out[0] = e;
+            ctl->out[1] = m;
+            ctl->iout[0] = mixbad;
+            ctl->iout[1] = bad;
+        }
+        return;
+    }
+    if (a.mode == kModeSnapshot) {
+        double v[5];
+        if (!snapshot(a, red, st.cur, v)) return;
+        double e, m;
+        bool mixbad, bad;
+        if (!phase_energy(a, red, st.cur, e, m, mixbad, bad)) return;
+        if (leader) {
+            for (int k = 0; k < 5; ++k) ctl->out[k] = v[k];
+            ctl->out[5] = m;
+            ctl->out[6] = e;
+            ctl->iout[0] = mixbad;
+        }
+        return;
+    }
+    if (a.mode == kModeMaybeShift) {
+        int rows = 0;
+        if (!maybe_shift(a, red, st, rows)) return;
+        if (leader) {
+            ctl->S = st.S;
+            ctl->cur = st.cur;
+            ctl->energy_valid = st.cache_valid ? 1 : 0;
+            ctl->iout[0] = rows;
+        }
+        return;
+    }
+}
+
+}  // namespace pearl_gpu
+
+// ====================================================================== host side
+using namespace pearl_gpu;
+
+struct pearl_gpu_ctx {
+    int device = 0;
+    int nx = 0, ny = 0, pitch = 0;
+    cudaStream_t stream = nullptr;
+    pearl_params params{};
+    DevParams P{};
+    DevBufs B{};
+    double* slab = nullptr;
+    Ctl* d_ctl = nullptr;
+    Ctl* h_ctl = nullptr;  // pinned
+    double* h_stage = nullptr;  // pinned staging of one plane-set
+    size_t stage_elems = 0;
+    int grid = 0;
+    long long launches = 0;
+    double last_ms = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string error;
+};
+
+namespace {
+
+const char* why_text(int why) {
+    switch (why) {
+        case PEARL_WHY_PHASE_INCREMENT: return "phase increment";
+        case PEARL_WHY_LINEAR_CLOSURE: return "linear/closure";
+        case PEARL_WHY_BOUNDS: return "composition/phase bounds";
+        case PEARL_WHY_MASS: return "mass conservation";
+        case PEARL_WHY_ENERGY: return "free-energy increase";
+        default: return "";
+    }
+}
+
+int fail(pearl_gpu_ctx* ctx, int status, const std::string& msg) {
+    if (ctx) ctx->error = msg;
+    return status;
+}
+
+int cuda_fail(pearl_gpu_ctx* ctx, cudaError_t e, const char* what) {
+    return fail(ctx, PEARL_ERR_CUDA, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+#define PG_CUDA(ctx, call)                                  \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+bool valid_params(const pearl_params* p) {
+    for (int i = 0; i < 3; ++i) {
+        // Parabola::validate (pearl_serial.cpp:76-79)
+        if (!std::isfinite(p->A[i]) || !std::isfinite(p->B[i]) || !std::isfinite(p->C[i]) || !std::isfinite(p->D[i]) ||
+            p->A[i] <= 0.0 || p->D[i] < 0.0)
+            return false;
+        if (!(p->tau[i] > 0) || !std::isfinite(p->tau[i])) return false;
+    }
+    // InterfaceParameters::validate / PhaseParameters::validate (:414-419, :522-529)
+    if (!(p->epsilon > 0) || !(p->sigma > 0) || p->triple < 0 || !std::isfinite(p->epsilon) ||
+        !std::isfinite(p->sigma) || !std::isfinite(p->triple))
+        return false;
+    if (!(p->Vm > 0) || !std::isfinite(p->Vm)) return false;
+    if (!(p->dx > 0) || !(p->dy > 0) || !std::isfinite(p->dx + p->dy)) return false;
+    if (p->cg_max < 0 || p->max_retries < 0) return false;
+    return true;
+}
+
+double host_psi(const pearl_params* p, int a, double mu) {
+    const double d = mu - p->B[a];
+    return std::fma(-0.25 / p->A[a], d * d, p->C[a]);
+}
+
+void fill_dev_params(pearl_gpu_ctx* ctx) {
+    const pearl_params* p = &ctx->params;
+    DevParams& P = ctx->P;
+    P.nx = ctx->nx;
+    P.ny = ctx->ny;
+    P.pitch = ctx->pitch;
+    P.ntx = (ctx->nx + kTileX - 1) / kTileX;
+    P.nty = (ctx->ny + kTileY - 1) / kTileY;
+    P.ntiles = P.ntx * P.nty;
+    P.dx = p->dx;
+    P.dy = p->dy;
+    P.dx2 = p->dx * p->dx;
+    P.dy2 = p->dy * p->dy;
+    P.Vm = p->Vm;
+    P.eps = p->epsilon;
+    const double pi = std::acos(-1.);
+    P.obs = 16 * p->sigma / (pi * pi * p->epsilon);
+    P.tr = p->triple / p->epsilon;
+    P.two_eps_sigma = 2 * p->epsilon * p->sigma;
+    P.eps_sigma = p->epsilon * p->sigma;
+    double tmin = p->tau[0];
+    for (int i = 0; i < 3; ++i) {
+        P.tau[i] = p->tau[i];
+        if (p->tau[i] < tmin) tmin = p->tau[i];
+        P.A[i] = p->A[i];
+        P.B[i] = p->B[i];
+        P.C[i] = p->C[i];
+        P.D[i] = p->D[i];
+        P.chi_p[i] = 1.0 / (2.0 * p->A[i]);
+        P.neg_q_A[i] = -0.25 / p->A[i];
+        P.two_A[i] = 2.0 * p->A[i];
+    }
+    P.tau_min = tmin;
+    P.mu_ref = p->mu_reference;
+    P.psi_t[0] = host_psi(p, 0, p->mu_reference) - host_psi(p, 2, p->mu_reference);
+    P.psi_t[1] = host_psi(p, 1, p->mu_reference) - host_psi(p, 2, p->mu_reference);
+    P.psi_t[2] = 0;
+    P.dt_max = p->dt_max;
+    P.dt_min = p->dt_min;
+    P.max_phase_change = p->max_phase_change;
+    P.cg_rtol = p->cg_rtol;
+    P.cg_atol = p->cg_atol;
+    P.closure_tol = p->closure_tol;
+    P.energy_rtol = p->energy_rtol;
+    P.energy_atol = p->energy_atol;
+    const int gxgy = ctx->nx * ctx->ny;
+    P.mass_scale = gxgy * p->dx * p->dy * 1e-6;
+    P.energy_scale = p->sigma * std::max(ctx->nx * p->dx, ctx->ny * p->dy);
+    P.cg_max = p->cg_max;
+    P.max_retries = p->max_retries;
+    P.check_energy = p->check_energy;
+    P.phase_only = p->phase_only;
+}
+
+int pull_ctl(pearl_gpu_ctx* ctx) {
+    PG_CUDA(ctx, cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PEARL_OK;
+}
+
+int push_ctl(pearl_gpu_ctx* ctx) {
+    PG_CUDA(ctx, cudaMemcpyAsync(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, ctx->stream));
+    return PEARL_OK;
+}
+
+// Launch the persistent kernel in `mode`; on return h_ctl holds the device
+// control block.  Maps the device status to the reference's messages.
+int launch(pearl_gpu_ctx* ctx, KArgs& args) {
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    ctx->h_ctl->status = 0;
+    ctx->h_ctl->why = 0;
+    ctx->h_ctl->bar_count = 0;
+    int rc = push_ctl(ctx);
+    if (rc) return rc;
+    args.P = ctx->P;
+    args.B = ctx->B;
+    void* kargs[] = {&args};
+    PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(ctx->grid), dim3(kThreads), kargs, 0,
+                                             ctx->stream));
+    ctx->launches++;
+    PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    rc = pull_ctl(ctx);
+    if (rc) return rc;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_ms = ms;
+    const int st = ctx->h_ctl->status;
+    if (st == PEARL_OK) return PEARL_OK;
+    ctx->h_ctl->energy_valid = 0;
+    switch (st) {
+        case PEARL_ERR_INVALID_ADVANCE_TIME: return fail(ctx, st, "invalid advance time");
+        case PEARL_ERR_REJECTED_BELOW_DT_MIN:
+            return fail(ctx, st, std::string("step rejected below dt_min: ") + why_text(ctx->h_ctl->why));
+        case PEARL_ERR_RETRY_LIMIT: return fail(ctx, st, std::string("step retry limit: ") + why_text(ctx->h_ctl->why));
+        case PEARL_ERR_MIXTURE: return fail(ctx, st, "Invalid mixture coefficients");
+        case PEARL_ERR_SIMPLEX: return fail(ctx, st, "Simplex projection failed");
+        case PEARL_ERR_MAX_STEPS: return fail(ctx, st, "configured max_steps reached before end_time");
+        case PEARL_ERR_UNSAFE_SHIFT: return fail(ctx, st, "unsafe shift: removed strip contains gamma");
+        case PEARL_ERR_NONFINITE_CARBON: return fail(ctx, st, "Nonfinite total carbon");
+        case PEARL_ERR_DEVICE_WAIT:
+            // a grid barrier gave up waiting: reset the barrier words before any further launch
+            ctx->h_ctl->bar_count = 0;
+            push_ctl(ctx);
+            return fail(ctx, st, "device grid barrier wait exceeded its limit");
+        default: return fail(ctx, st, "invalid argument");
+    }
+}
+
+size_t plane_elems(const pearl_gpu_ctx* ctx) { return (size_t)ctx->pitch * ctx->ny; }
+
+// AoS host (ny,nx,3) + two scalar fields <-> padded SoA device planes
+int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* carbon, const double* mu) {
+    const size_t n = (size_t)ctx->nx * ctx->ny;
+    const size_t pe = plane_elems(ctx);
+    double* st = ctx->h_stage;
+    if (phi) {
+        for (int a = 0; a < 3; ++a) {
+            for (int y = 0; y < ctx->ny; ++y)
+                for (int x = 0; x < ctx->nx; ++x)
+                    st[(size_t)a * pe + (size_t)y * ctx->pitch + x] = phi[((size_t)y * ctx->nx + x) * 3 + a];
+        }
+    }
+    if (carbon)
+        for (int y = 0; y < ctx->ny; ++y)
+            std::memcpy(st + 3 * pe + (size_t)y * ctx->pitch, carbon + (size_t)y * ctx->nx, sizeof(double) * ctx->nx);
+    if (mu)
+        for (int y = 0; y < ctx->ny; ++y)
+            std::memcpy(st + 4 * pe + (size_t)y * ctx->pitch, mu + (size_t)y * ctx->nx, sizeof(double) * ctx->nx);
+    (void)n;
+    if (phi)
+        for (int a = 0; a < 3; ++a)
+            PG_CUDA(ctx, cudaMemcpyAsync(ctx->B.phi[set][a], st + (size_t)a * pe, pe * sizeof(double),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+    if (carbon)
+        PG_CUDA(ctx, cudaMemcpyAsync(ctx->B.c[set], st + 3 * pe, pe * sizeof(double), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    if (mu)
+        PG_CUDA(ctx, cudaMemcpyAsync(ctx->B.mu[set], st + 4 * pe, pe * sizeof(double), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PEARL_OK;
+}
+
+int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, double* mu) {
+    const size_t pe = plane_elems(ctx);
+    double* st = ctx->h_stage;
+    if (phi)
+        for (int a = 0; a < 3; ++a)
+            PG_CUDA(ctx, cudaMemcpyAsync(st + (size_t)a * pe, ctx->B.phi[set][a], pe * sizeof(double),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    if (carbon)
+        PG_CUDA(ctx, cudaMemcpyAsync(st + 3 * pe, ctx->B.c[set], pe * sizeof(double), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    if (mu)
+        PG_CUDA(ctx, cudaMemcpyAsync(st + 4 * pe, ctx->B.mu[set], pe * sizeof(double), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (phi)
+        for (int y = 0; y < ctx->ny; ++y)
+            for (int x = 0; x < ctx->nx; ++x)
+                for (int a = 0; a < 3; ++a)
+                    phi[((size_t)y * ctx->nx + x) * 3 + a] = st[(size_t)a * pe + (size_t)y * ctx->pitch + x];
+    if (carbon)
+        for (int y = 0; y < ctx->ny; ++y)
+            std::memcpy(carbon + (size_t)y * ctx->nx, st + 3 * pe + (size_t)y * ctx->pitch, sizeof(double) * ctx->nx);
+    if (mu)
+        for (int y = 0; y < ctx->ny; ++y)
+            std::memcpy(mu + (size_t)y * ctx->nx, st + 4 * pe + (size_t)y * ctx->pitch, sizeof(double) * ctx->nx);
+    return PEARL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pearl_gpu_status_string(int status) {
+    switch (status) {
+        case PEARL_OK: return "ok";
+        case PEARL_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case PEARL_ERR_CUDA: return "CUDA error";
+        case PEARL_ERR_INVALID_ADVANCE_TIME: return "invalid advance time";
+        case PEARL_ERR_REJECTED_BELOW_DT_MIN: return "step rejected below dt_min";
+        case PEARL_ERR_RETRY_LIMIT: return "step retry limit";
+        case PEARL_ERR_MIXTURE: return "Invalid mixture coefficients";
+        case PEARL_ERR_SIMPLEX: return "Simplex projection failed";
+        case PEARL_ERR_MAX_STEPS: return "configured max_steps reached before end_time";
+        case PEARL_ERR_DEVICE_WAIT: return "device wait limit exceeded";
+        case PEARL_ERR_UNSAFE_SHIFT: return "unsafe shift: removed strip contains gamma";
+        case PEARL_ERR_NONFINITE_CARBON: return "Nonfinite total carbon";
+        case PEARL_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* pearl_gpu_last_error(const pearl_gpu_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pearl_gpu_ctx** out) {
+    if (!out) return PEARL_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!params || nx < 3 || ny < 2 || !valid_params(params)) return PEARL_ERR_INVALID_ARGUMENT;
+    if ((long long)nx * ny > 2000000000LL) return PEARL_ERR_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return PEARL_ERR_NO_DEVICE;
+    pearl_gpu_ctx* ctx = new pearl_gpu_ctx();
+    ctx->device = device;
+    ctx->nx = nx;
+    ctx->ny = ny;
+    ctx->pitch = (nx + 31) / 32 * 32;
+    ctx->params = *params;
+    auto bail = [&](int rc) {
+        pearl_gpu_destroy(ctx);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    int coop = 0, sms = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (!coop) return bail(PEARL_ERR_NO_DEVICE);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads, 0) != cudaSuccess ||
+        per_sm < 1)
+        return bail(PEARL_ERR_CUDA);
+    fill_dev_params(ctx);
+    ctx->grid = std::max(1, std::min(per_sm * sms, ctx->P.ntiles));
+    // state: 2 x (3 phi + c + mu); work: K chi icpt diag x r z p0 p1 Ap  -> 20 planes
+    const size_t pe = plane_elems(ctx);
+    const int nplanes = 20;
+    const size_t part = (size_t)2 * ctx->grid * kMaxRed;
+    if (cudaMalloc(&ctx->slab, (nplanes * pe + part) * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    if (cudaMemset(ctx->slab, 0, (nplanes * pe + part) * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    double* q = ctx->slab;
+    for (int s = 0; s < 2; ++s) {
+        for (int a = 0; a < 3; ++a, q += pe) ctx->B.phi[s][a] = q;
+        ctx->B.c[s] = q;
+        q += pe;
+        ctx->B.mu[s] = q;
+        q += pe;
+    }
+    ctx->B.K = q; q += pe;
+    ctx->B.chi = q; q += pe;
+    ctx->B.icpt = q; q += pe;
+    ctx->B.diag = q; q += pe;
+    ctx->B.x = q; q += pe;
+    ctx->B.r = q; q += pe;
+    ctx->B.z = q; q += pe;
+    ctx->B.p[0] = q; q += pe;
+    ctx->B.p[1] = q; q += pe;
+    ctx->B.Ap = q; q += pe;
+    ctx->B.part = q;
+    if (cudaMalloc(&ctx->d_ctl, sizeof(Ctl)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    if (cudaMallocHost(&ctx->h_ctl, sizeof(Ctl)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    std::memset(ctx->h_ctl, 0, sizeof(Ctl));
+    ctx->B.ctl = ctx->d_ctl;
+    ctx->stage_elems = 5 * pe;
+    if (cudaMallocHost(&ctx->h_stage, ctx->stage_elems * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+        return bail(PEARL_ERR_CUDA);
+    if (cudaMemcpy(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(PEARL_ERR_CUDA);
+    *out = ctx;
+    return PEARL_OK;
+}
+
+void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->slab) cudaFree(ctx->slab);
+    if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+    if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    delete ctx;
+}
+
+int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    ctx->stream = (cudaStream_t)stream;
+    return PEARL_OK;
+}
+
+int pearl_gpu_set_params(pearl_gpu_ctx* ctx, const pearl_params* params) {
+    if (!ctx || !params || !valid_params(params)) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid parameters");
+    ctx->params = *params;
+    fill_dev_params(ctx);
+    ctx->h_ctl->energy_valid = 0;
+    return push_ctl(ctx);
+}
+
+int pearl_gpu_upload(pearl_gpu_ctx* ctx, const double* phi, const double* carbon, const double* mu,
+                     const pearl_scalars* scalars) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    int rc = upload_set(ctx, ctx->h_ctl->cur, phi, carbon, mu);
+    if (rc) return rc;
+    if (scalars) ctx->h_ctl->S = *scalars;
+    ctx->h_ctl->energy_valid = 0;
+    rc = push_ctl(ctx);
+    if (rc) return rc;
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PEARL_OK;
+}
+
+int pearl_gpu_download(pearl_gpu_ctx* ctx, double* phi, double* carbon, double* mu, pearl_scalars* scalars) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    int rc = download_set(ctx, ctx->h_ctl->cur, phi, carbon, mu);
+    if (rc) return rc;
+    if (scalars) *scalars = ctx->h_ctl->S;
+    return PEARL_OK;
+}
+
+int pearl_gpu_get_scalars(pearl_gpu_ctx* ctx, pearl_scalars* scalars) {
+    if (!ctx || !scalars) return PEARL_ERR_INVALID_ARGUMENT;
+    *scalars = ctx->h_ctl->S;
+    return PEARL_OK;
+}
+
+int pearl_gpu_set_scalars(pearl_gpu_ctx* ctx, const pearl_scalars* scalars) {
+    if (!ctx || !scalars) return PEARL_ERR_INVALID_ARGUMENT;
+    ctx->h_ctl->S = *scalars;
+    int rc = push_ctl(ctx);
+    if (rc) return rc;
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PEARL_OK;
+}
+
+int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_report* report) {
+    if (!ctx || !limits || limits->max_steps < 1) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid run limits");
+    KArgs a{};
+    a.mode = kModeRun;
+    a.L = *limits;
+    int rc = launch(ctx, a);
+    if (report) {
+        report->steps = ctx->h_ctl->steps;
+        report->cg_total = ctx->h_ctl->cg_total;
+        report->cg_peak = ctx->h_ctl->cg_peak;
+        report->reached_stop = ctx->h_ctl->reached_stop;
+        report->last = ctx->h_ctl->last;
+    }
+    return rc;
+}
+
+int pearl_gpu_advance(pearl_gpu_ctx* ctx, double stop_time, pearl_step_info* out) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    pearl_run_limits L;
+    L.max_steps = 1;
+    L.config_max_steps = 0x7fffffffffffffffLL;
+    L.stop_time = stop_time;
+    L.end_time = INFINITY;
+    L.output_eps = 0;
+    pearl_run_report rep;
+    int rc = pearl_gpu_run(ctx, &L, &rep);
+    if (rc == PEARL_OK && rep.steps != 1) return fail(ctx, PEARL_ERR_INVALID_ADVANCE_TIME, "invalid advance time");
+    if (out) *out = rep.last;
+    return rc;
+}
+
+int pearl_gpu_maybe_shift(pearl_gpu_ctx* ctx, double trigger, double target, double c_gamma, int* rows) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeMaybeShift;
+    a.shift_trigger = trigger;
+    a.shift_target = target;
+    a.shift_c_gamma = c_gamma;
+    int rc = launch(ctx, a);
+    if (rows) *rows = rc == PEARL_OK ? ctx->h_ctl->iout[0] : 0;
+    return rc;
+}
+
+int pearl_gpu_snapshot(pearl_gpu_ctx* ctx, pearl_diag* out) {
+    if (!ctx || !out) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeSnapshot;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
+    const Ctl* h = ctx->h_ctl;
+    out->c_min = h->out[0];
+    out->c_max = h->out[1];
+    out->mu_min = h->out[2];
+    out->mu_max = h->out[3];
+    out->phi_sum_error = h->out[4];
+    out->mass = h->out[5];
+    out->energy = h->out[6];
+    out->ledger = out->mass + h->S.carbon_removed - h->S.carbon_added - h->S.initial_carbon;
+    return PEARL_OK;
+}
+
+int pearl_gpu_propose_phi(pearl_gpu_ctx* ctx, double dt, double* max_change) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModePropose;
+    a.dt = dt;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ctx->h_ctl->iout[1]) return fail(ctx, PEARL_ERR_SIMPLEX, "Simplex projection failed");
+    if (max_change) *max_change = ctx->h_ctl->out[0];
+    return PEARL_OK;
+}
+
+int pearl_gpu_upload_trial_phi(pearl_gpu_ctx* ctx, const double* phi) {
+    if (!ctx || !phi) return PEARL_ERR_INVALID_ARGUMENT;
+    int rc = upload_set(ctx, ctx->h_ctl->cur ^ 1, phi, nullptr, nullptr);
+    if (rc) return rc;
+    KArgs a{};
+    a.mode = kModeMix;
+    rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
+    return PEARL_OK;
+}
+
+int pearl_gpu_implicit_diffusion(pearl_gpu_ctx* ctx, double dt, int* ok, int* iterations, double* residual,
+                                 double* closure) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeDiffusion;
+    a.dt = dt;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ok) *ok = ctx->h_ctl->iout[0];
+    if (iterations) *iterations = ctx->h_ctl->iout[1];
+    if (residual) *residual = ctx->h_ctl->out[0];
+    if (closure) *closure = ctx->h_ctl->out[1];
+    return PEARL_OK;
+}
+
+int pearl_gpu_download_trial(pearl_gpu_ctx* ctx, double* phi, double* carbon, double* mu) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    return download_set(ctx, ctx->h_ctl->cur ^ 1, phi, carbon, mu);
+}
+
+int pearl_gpu_energy_mass(pearl_gpu_ctx* ctx, double* energy, double* mass) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeEnergy;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
+    if (energy) *energy = ctx->h_ctl->out[0];
+    if (mass) *mass = ctx->h_ctl->out[1];
+    return PEARL_OK;
+}
+
+int pearl_gpu_valid_state(pearl_gpu_ctx* ctx, int* valid) {
+    if (!ctx || !valid) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeValid;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    *valid = ctx->h_ctl->iout[1] ? 0 : 1;
+    return PEARL_OK;
+}
+
+int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* launches, int* grid_blocks, double* last_ms) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    if (launches) *launches = ctx->launches;
+    if (grid_blocks) *grid_blocks = ctx->grid;
+    if (last_ms) *last_ms = ctx->last_ms;
+    return PEARL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,286 @@
+"""Python view of libpearl_gpu.so, the B200 hot path of the Pearl pearlite solver.
+
+This module only binds the C ABI declared in ``include/pearl_gpu.h`` with
+ctypes; all arithmetic runs in the CUDA library.  There is no CPU fallback:
+importing the binding fails loudly when the library has not been built, and
+creating a context fails when no CUDA device is present.
+
+Host arrays use the reference's gathered layout: ``phi[ny, nx, 3]`` (alpha,
+theta, gamma), ``carbon[ny, nx]``, ``mu[ny, nx]``, float64, C-contiguous.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .build import LIB
+
+D = C.c_double
+DP = C.POINTER(C.c_double)
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "invalid advance time",
+    4: "step rejected below dt_min", 5: "step retry limit", 6: "Invalid mixture coefficients",
+    7: "Simplex projection failed", 8: "configured max_steps reached before end_time",
+    9: "device wait limit exceeded", 10: "unsafe shift: removed strip contains gamma",
+    11: "Nonfinite total carbon", 12: "no CUDA device",
+}
+
+
+class PearlParams(C.Structure):
+    """pearl_params (include/pearl_gpu.h)."""
+
+    _fields_ = [
+        ("A", D * 3), ("B", D * 3), ("C", D * 3), ("D", D * 3),
+        ("Vm", D), ("epsilon", D), ("sigma", D), ("triple", D),
+        ("tau", D * 3),
+        ("dx", D), ("dy", D),
+        ("dt_max", D), ("dt_min", D), ("max_phase_change", D),
+        ("cg_rtol", D), ("cg_atol", D), ("closure_tol", D),
+        ("energy_rtol", D), ("energy_atol", D),
+        ("cg_max", C.c_int), ("max_retries", C.c_int), ("check_energy", C.c_int), ("phase_only", C.c_int),
+        ("mu_reference", D),
+    ]
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "PearlParams":
+        p = cls()
+        for name, _ in cls._fields_:
+            v = d[name]
+            if isinstance(getattr(p, name), C.Array):
+                arr = getattr(p, name)
+                for i in range(3):
+                    arr[i] = float(v[i])
+            else:
+                setattr(p, name, v)
+        return p
+
+
+class PearlScalars(C.Structure):
+    """pearl_scalars: the scalar members of pearl::State."""
+
+    _fields_ = [
+        ("time", D), ("dt", D), ("shift_distance", D), ("initial_carbon", D),
+        ("carbon_added", D), ("carbon_removed", D),
+        ("step", C.c_longlong), ("shifts", C.c_longlong), ("rejected", C.c_longlong),
+    ]
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "PearlScalars":
+        s = cls()
+        for name, _ in cls._fields_:
+            setattr(s, name, d[name])
+        return s
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class PearlStepInfo(C.Structure):
+    """pearl_step_info: pearl::StepInfo."""
+
+    _fields_ = [
+        ("accepted_dt", D), ("max_phase_change", D), ("linear_residual", D), ("closure", D),
+        ("energy_change", D), ("cg_iterations", C.c_int), ("retries", C.c_int),
+    ]
+
+
+class PearlRunLimits(C.Structure):
+    _fields_ = [("max_steps", C.c_longlong), ("config_max_steps", C.c_longlong), ("stop_time", D),
+                ("end_time", D), ("output_eps", D)]
+
+
+class PearlRunReport(C.Structure):
+    _fields_ = [("steps", C.c_longlong), ("cg_total", C.c_longlong), ("cg_peak", C.c_int),
+                ("reached_stop", C.c_int), ("last", PearlStepInfo)]
+
+
+class PearlDiag(C.Structure):
+    _fields_ = [(n, D) for n in ("c_min", "c_max", "mu_min", "mu_max", "phi_sum_error", "mass", "ledger", "energy")]
+
+
+EXPORTS = [
+    "pearl_gpu_create", "pearl_gpu_destroy", "pearl_gpu_set_stream", "pearl_gpu_set_params", "pearl_gpu_upload",
+    "pearl_gpu_download", "pearl_gpu_get_scalars", "pearl_gpu_set_scalars", "pearl_gpu_advance", "pearl_gpu_run",
+    "pearl_gpu_maybe_shift", "pearl_gpu_snapshot", "pearl_gpu_propose_phi", "pearl_gpu_upload_trial_phi",
+    "pearl_gpu_implicit_diffusion", "pearl_gpu_download_trial", "pearl_gpu_energy_mass", "pearl_gpu_valid_state",
+    "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats",
+]
+
+_lib = None
+
+
+def library(path: Path | None = None) -> C.CDLL:
+    """Load libpearl_gpu.so; raises if it is missing (build with __graft_entry__.build())."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB
+    if not p.exists():
+        raise ImportError(f"{p} is missing: the CUDA library must be built (python -m pearl_gpu.build)")
+    L = C.CDLL(str(p))
+    V = C.c_void_p
+    L.pearl_gpu_create.argtypes = [C.POINTER(PearlParams), C.c_int, C.c_int, C.c_int, C.POINTER(V)]
+    L.pearl_gpu_destroy.argtypes = [V]
+    L.pearl_gpu_destroy.restype = None
+    L.pearl_gpu_set_stream.argtypes = [V, V]
+    L.pearl_gpu_set_params.argtypes = [V, C.POINTER(PearlParams)]
+    L.pearl_gpu_upload.argtypes = [V, DP, DP, DP, C.POINTER(PearlScalars)]
+    L.pearl_gpu_download.argtypes = [V, DP, DP, DP, C.POINTER(PearlScalars)]
+    L.pearl_gpu_get_scalars.argtypes = [V, C.POINTER(PearlScalars)]
+    L.pearl_gpu_set_scalars.argtypes = [V, C.POINTER(PearlScalars)]
+    L.pearl_gpu_advance.argtypes = [V, D, C.POINTER(PearlStepInfo)]
+    L.pearl_gpu_run.argtypes = [V, C.POINTER(PearlRunLimits), C.POINTER(PearlRunReport)]
+    L.pearl_gpu_maybe_shift.argtypes = [V, D, D, D, C.POINTER(C.c_int)]
+    L.pearl_gpu_snapshot.argtypes = [V, C.POINTER(PearlDiag)]
+    L.pearl_gpu_propose_phi.argtypes = [V, D, DP]
+    L.pearl_gpu_upload_trial_phi.argtypes = [V, DP]
+    L.pearl_gpu_implicit_diffusion.argtypes = [V, D, C.POINTER(C.c_int), C.POINTER(C.c_int), DP, DP]
+    L.pearl_gpu_download_trial.argtypes = [V, DP, DP, DP]
+    L.pearl_gpu_energy_mass.argtypes = [V, DP, DP]
+    L.pearl_gpu_valid_state.argtypes = [V, C.POINTER(C.c_int)]
+    L.pearl_gpu_status_string.argtypes = [C.c_int]
+    L.pearl_gpu_status_string.restype = C.c_char_p
+    L.pearl_gpu_last_error.argtypes = [V]
+    L.pearl_gpu_last_error.restype = C.c_char_p
+    L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
+    if path is None:
+        _lib = L
+    return L
+
+
+class PearlError(RuntimeError):
+    """A non-zero pearl_status; ``str()`` is the reference-style message."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message or STATUS.get(status, f"status {status}"))
+        self.status = status
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(DP)
+
+
+class Context:
+    """One device-resident domain (pearl_gpu_ctx)."""
+
+    def __init__(self, params: dict | PearlParams, nx: int, ny: int, device: int = 0, stream: int | None = None):
+        self.lib = library()
+        self.nx, self.ny = nx, ny
+        self.params = params if isinstance(params, PearlParams) else PearlParams.from_dict(params)
+        h = C.c_void_p()
+        rc = self.lib.pearl_gpu_create(C.byref(self.params), nx, ny, device, C.byref(h))
+        if rc:
+            raise PearlError(rc, f"pearl_gpu_create failed: {STATUS.get(rc, rc)}")
+        self.h = h
+        if stream is not None:
+            self._check(self.lib.pearl_gpu_set_stream(self.h, C.c_void_p(stream)))
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise PearlError(rc, self.lib.pearl_gpu_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.pearl_gpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    # ---- state transfer (Domain::load_global / gather)
+    def upload(self, phi, carbon, mu, scalars: dict | PearlScalars | None = None) -> None:
+        s = None
+        if scalars is not None:
+            s = scalars if isinstance(scalars, PearlScalars) else PearlScalars.from_dict(scalars)
+        self._check(self.lib.pearl_gpu_upload(self.h, _p(phi), _p(carbon), _p(mu), C.byref(s) if s else None))
+
+    def download(self):
+        phi = np.empty((self.ny, self.nx, 3))
+        carbon = np.empty((self.ny, self.nx))
+        mu = np.empty((self.ny, self.nx))
+        s = PearlScalars()
+        self._check(self.lib.pearl_gpu_download(self.h, _p(phi), _p(carbon), _p(mu), C.byref(s)))
+        return phi, carbon, mu, s
+
+    def scalars(self) -> PearlScalars:
+        s = PearlScalars()
+        self._check(self.lib.pearl_gpu_get_scalars(self.h, C.byref(s)))
+        return s
+
+    def set_scalars(self, s: dict | PearlScalars) -> None:
+        s = s if isinstance(s, PearlScalars) else PearlScalars.from_dict(s)
+        self._check(self.lib.pearl_gpu_set_scalars(self.h, C.byref(s)))
+
+    # ---- hot path
+    def advance(self, stop_time: float = 1e300) -> PearlStepInfo:
+        info = PearlStepInfo()
+        self._check(self.lib.pearl_gpu_advance(self.h, stop_time, C.byref(info)))
+        return info
+
+    def run(self, max_steps: int, stop_time: float = 1e300, end_time: float = 1e300, output_eps: float = 0.0,
+            config_max_steps: int = 2**62) -> PearlRunReport:
+        lim = PearlRunLimits(max_steps, config_max_steps, stop_time, end_time, output_eps)
+        rep = PearlRunReport()
+        self._check(self.lib.pearl_gpu_run(self.h, C.byref(lim), C.byref(rep)))
+        return rep
+
+    def maybe_shift(self, trigger: float, target: float, c_gamma: float) -> int:
+        rows = C.c_int(0)
+        self._check(self.lib.pearl_gpu_maybe_shift(self.h, trigger, target, c_gamma, C.byref(rows)))
+        return rows.value
+
+    def snapshot(self) -> PearlDiag:
+        d = PearlDiag()
+        self._check(self.lib.pearl_gpu_snapshot(self.h, C.byref(d)))
+        return d
+
+    # ---- single functions of the hot path
+    def propose_phi(self, dt: float) -> float:
+        ch = D()
+        self._check(self.lib.pearl_gpu_propose_phi(self.h, dt, C.byref(ch)))
+        return ch.value
+
+    def upload_trial_phi(self, phi) -> None:
+        self._check(self.lib.pearl_gpu_upload_trial_phi(self.h, _p(phi)))
+
+    def implicit_diffusion(self, dt: float):
+        ok, it = C.c_int(), C.c_int()
+        res, clo = D(), D()
+        self._check(self.lib.pearl_gpu_implicit_diffusion(self.h, dt, C.byref(ok), C.byref(it), C.byref(res),
+                                                          C.byref(clo)))
+        return dict(ok=ok.value, it=it.value, residual=res.value, closure=clo.value)
+
+    def download_trial(self):
+        phi = np.empty((self.ny, self.nx, 3))
+        carbon = np.empty((self.ny, self.nx))
+        mu = np.empty((self.ny, self.nx))
+        self._check(self.lib.pearl_gpu_download_trial(self.h, _p(phi), _p(carbon), _p(mu)))
+        return phi, carbon, mu
+
+    def energy_mass(self):
+        e, m = D(), D()
+        self._check(self.lib.pearl_gpu_energy_mass(self.h, C.byref(e), C.byref(m)))
+        return e.value, m.value
+
+    def valid_state(self) -> bool:
+        v = C.c_int()
+        self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
+        return bool(v.value)
+
+    def stats(self):
+        n, g, ms = C.c_longlong(), C.c_int(), D()
+        self._check(self.lib.pearl_gpu_stats(self.h, C.byref(n), C.byref(g), C.byref(ms)))
+        return dict(launches=n.value, grid=g.value, last_ms=ms.value)

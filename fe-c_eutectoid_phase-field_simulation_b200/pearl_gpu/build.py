@@ -1,0 +1,75 @@
+"""In-tree build of libpearl_gpu.so (sm_100a) and the pearl_gpu host executable.
+
+nvcc cross-compiles for sm_100a without a GPU, so this runs on any host with
+the CUDA 12.9 toolchain.  Outputs go to ``<package>/build/`` (git-ignored, but
+shipped with the repository snapshot to GPU hosts).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent.parent  # fe-c_eutectoid_phase-field_simulation_b200/
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+HOST = PKG / "host"
+INCLUDE = ROOT / "include"
+BUILD = PKG / "build"
+LIB = BUILD / "libpearl_gpu.so"
+CLI = BUILD / "pearl_gpu"
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+# FP64 path: -fmad=false keeps every multiply and add separately rounded, as in
+# the reference built for plain x86-64, so per-cell results match bitwise.
+CU_SOURCES = {
+    "pearl_fp64.cu": ["-fmad=false"],
+}
+HOST_SOURCES: list[str] = []
+
+
+def _run(cmd: list[str]) -> None:
+    subprocess.run(cmd, check=True)
+
+
+def _newer(out: Path, inputs: list[Path]) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in inputs if p.exists())
+
+
+def sources() -> list[Path]:
+    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h"))
+    deps += list(HOST.glob("*.cpp")) + list(HOST.glob("*.hpp")) + list(INCLUDE.glob("*.h"))
+    return deps
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    deps = sources() + [Path(__file__)]
+    if force or _newer(LIB, deps):
+        objs = []
+        for name, extra in CU_SOURCES.items():
+            obj = BUILD / (Path(name).stem + ".o")
+            cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", *extra, "-Xcompiler", "-fPIC",
+                   f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / name), "-o", str(obj)]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            _run(cmd)
+            objs.append(obj)
+        for name in HOST_SOURCES:
+            obj = BUILD / (Path(name).stem + ".host.o")
+            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{HOST}",
+                  "-c", str(HOST / name), "-o", str(obj)])
+            objs.append(obj)
+        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(LIB)])
+    return LIB
+
+
+if __name__ == "__main__":
+    import sys
+
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,182 @@
+/*
+ * pearl_gpu.h — C ABI of libpearl_gpu.so, the B200 (sm_100a) implementation of
+ * the time-step hot path of the Pearl three-phase Fe-C pearlite phase-field
+ * solver.
+ *
+ * The reference has no plugin or FFI layer: its hot path is the internal C++
+ * call
+ *     StepInfo pearl::advance(const Domain&, State&, const Thermo&,
+ *                             const PhaseParameters&, const Controls&,
+ *                             double mu_reference, double stop_time)
+ * (pearl_serial.cpp:1119), called only from main's time loop
+ * (pearl_serial.cpp:2296-2316).  This header is that boundary in C: plain
+ * pointers and sizes, status codes instead of C++ exceptions, one device-
+ * resident domain per context.  Each entry point names the reference
+ * function or type it replaces.
+ *
+ * Conventions
+ *  - Host arrays use the reference's gathered global layout
+ *    (Domain::gather, pearl_serial.cpp:695-722): row-major (ny, nx), x fastest;
+ *    phase fractions interleaved per cell as (alpha, theta, gamma).
+ *    x (nx) is periodic, y (ny) has zero-flux walls.
+ *  - The library owns all device memory; the caller owns host buffers.
+ *  - Every call returns PEARL_OK (0) or a pearl_status code; the text of the
+ *    last error, formatted like the reference's exception messages, is
+ *    available from pearl_gpu_last_error().
+ *  - A context is bound to one CUDA device and one stream; calls on the same
+ *    context must not run concurrently from several host threads.
+ */
+#ifndef PEARL_GPU_H
+#define PEARL_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PEARL_GPU_ABI_VERSION 1
+
+/* Physics and numerical controls of one run.
+ * Replaces pearl::Thermo (pearl_serial.cpp:92), pearl::PhaseParameters
+ * (:517-531), pearl::Controls (:767-773), the grid spacings of pearl::Domain
+ * (:617) and the mu_reference argument of pearl::advance (:1119).
+ * Thermodynamics are the run-temperature parabolas f_p(c) = A c^2 + B c + C,
+ * phase index 0 alpha (ferrite), 1 theta (cementite), 2 gamma (austenite). */
+typedef struct pearl_params {
+    double A[3], B[3], C[3], D[3];
+    double Vm, epsilon, sigma, triple;
+    double tau[3]; /* tau_at, tau_ag, tau_tg */
+    double dx, dy;
+    double dt_max, dt_min, max_phase_change;
+    double cg_rtol, cg_atol, closure_tol;
+    double energy_rtol, energy_atol;
+    int cg_max, max_retries, check_energy, phase_only;
+    double mu_reference;
+} pearl_params;
+
+/* Scalar members of pearl::State (pearl_serial.cpp:758-764). */
+typedef struct pearl_scalars {
+    double time, dt, shift_distance, initial_carbon, carbon_added, carbon_removed;
+    long long step, shifts, rejected;
+} pearl_scalars;
+
+/* pearl::StepInfo (pearl_serial.cpp:774-777). */
+typedef struct pearl_step_info {
+    double accepted_dt, max_phase_change, linear_residual, closure, energy_change;
+    int cg_iterations, retries;
+} pearl_step_info;
+
+/* The contract of main's time loop (pearl_serial.cpp:2296-2316) for one call
+ * of pearl_gpu_run: advance until an output time, the end time, a step budget
+ * or an error, without returning to the host in between. */
+typedef struct pearl_run_limits {
+    long long max_steps;        /* accepted steps this call may take (>0) */
+    long long config_max_steps; /* Config::max_steps: error once step >= this */
+    double stop_time;           /* min(end_time, next_output) */
+    double end_time;            /* loop runs while time < end_time */
+    double output_eps;          /* 1e-12*max(end_time, output_dt): stop when time >= stop_time-eps */
+} pearl_run_limits;
+
+typedef struct pearl_run_report {
+    long long steps;        /* accepted steps taken by this call */
+    long long cg_total;     /* sum of StepInfo::cg_iterations */
+    int cg_peak;            /* max StepInfo::cg_iterations */
+    int reached_stop;       /* 1 if time >= stop_time - output_eps */
+    pearl_step_info last;   /* StepInfo of the last accepted step */
+} pearl_run_report;
+
+/* Output-time reductions of main's snapshot() (pearl_serial.cpp:2266-2281). */
+typedef struct pearl_diag {
+    double c_min, c_max, mu_min, mu_max, phi_sum_error, mass, ledger, energy;
+} pearl_diag;
+
+typedef enum pearl_status {
+    PEARL_OK = 0,
+    PEARL_ERR_INVALID_ARGUMENT = 1,
+    PEARL_ERR_CUDA = 2,
+    PEARL_ERR_INVALID_ADVANCE_TIME = 3,   /* "invalid advance time" (:1121) */
+    PEARL_ERR_REJECTED_BELOW_DT_MIN = 4,  /* "step rejected below dt_min: <why>" (:1171) */
+    PEARL_ERR_RETRY_LIMIT = 5,            /* "step retry limit: <why>" (:1173) */
+    PEARL_ERR_MIXTURE = 6,                /* "Invalid mixture coefficients" (:136) */
+    PEARL_ERR_SIMPLEX = 7,                /* "Simplex projection failed" (:505) */
+    PEARL_ERR_MAX_STEPS = 8,              /* "configured max_steps reached before end_time" (:2302) */
+    PEARL_ERR_DEVICE_WAIT = 9,            /* a bounded device-side wait ran out (no reference counterpart) */
+    PEARL_ERR_UNSAFE_SHIFT = 10,          /* "unsafe shift: removed strip contains gamma" (:2068) */
+    PEARL_ERR_NONFINITE_CARBON = 11,      /* "Nonfinite total carbon" (:140) */
+    PEARL_ERR_NO_DEVICE = 12
+} pearl_status;
+
+/* Rejection reason <why> of the last attempt (pearl_serial.cpp:1133-1160). */
+typedef enum pearl_why {
+    PEARL_WHY_NONE = 0,
+    PEARL_WHY_PHASE_INCREMENT = 1,  /* "phase increment" */
+    PEARL_WHY_LINEAR_CLOSURE = 2,   /* "linear/closure" */
+    PEARL_WHY_BOUNDS = 3,           /* "composition/phase bounds" */
+    PEARL_WHY_MASS = 4,             /* "mass conservation" */
+    PEARL_WHY_ENERGY = 5            /* "free-energy increase" */
+} pearl_why;
+
+typedef struct pearl_gpu_ctx pearl_gpu_ctx;
+
+/* Allocate one device-resident domain of nx*ny cells on `device`
+ * (replaces pearl::Domain + pearl::State construction, pearl_serial.cpp:617, :763).
+ * nx >= 3 and ny >= 2 as in Domain's constructor (:618). */
+int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pearl_gpu_ctx** out);
+void pearl_gpu_destroy(pearl_gpu_ctx* ctx);
+
+/* Run all work of this context on `stream` (a cudaStream_t; NULL = legacy default). */
+int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream);
+
+/* Replace the run parameters (same grid); invalidates cached step energies. */
+int pearl_gpu_set_params(pearl_gpu_ctx* ctx, const pearl_params* params);
+
+/* Host -> device state (Domain::load_global, pearl_serial.cpp:725-736).
+ * phi_aos3[(y*nx+x)*3+a], carbon[y*nx+x], mu[y*nx+x]; scalars may be NULL. */
+int pearl_gpu_upload(pearl_gpu_ctx* ctx, const double* phi_aos3, const double* carbon, const double* mu,
+                     const pearl_scalars* scalars);
+/* Device -> host state (Domain::gather, pearl_serial.cpp:695-722); any pointer may be NULL. */
+int pearl_gpu_download(pearl_gpu_ctx* ctx, double* phi_aos3, double* carbon, double* mu, pearl_scalars* scalars);
+int pearl_gpu_get_scalars(pearl_gpu_ctx* ctx, pearl_scalars* scalars);
+int pearl_gpu_set_scalars(pearl_gpu_ctx* ctx, const pearl_scalars* scalars);
+
+/* One accepted step: pearl::advance (pearl_serial.cpp:1119-1174).  On error
+ * the state is unchanged and the status says why. */
+int pearl_gpu_advance(pearl_gpu_ctx* ctx, double stop_time, pearl_step_info* out);
+
+/* Many accepted steps in one device launch, deciding dt, retries and CG
+ * termination on the GPU (main's loop body, pearl_serial.cpp:2296-2306). */
+int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_report* report);
+
+/* Moving window (maybe_shift + shift_rows, pearl_serial.cpp:2023-2071).
+ * *rows receives the number of rows shifted (0 if the front is below trigger). */
+int pearl_gpu_maybe_shift(pearl_gpu_ctx* ctx, double shift_trigger, double shift_target, double shift_gamma_carbon,
+                          int* rows);
+
+/* Output-time reductions of snapshot() (pearl_serial.cpp:2266-2281). */
+int pearl_gpu_snapshot(pearl_gpu_ctx* ctx, pearl_diag* out);
+
+/* ---- single hot-path functions, for per-function parity checks ---- */
+/* propose_phi (pearl_serial.cpp:961-1002): writes the proposal into the trial buffer. */
+int pearl_gpu_propose_phi(pearl_gpu_ctx* ctx, double dt, double* max_change);
+/* Uploads phase fractions into the trial buffer (the trial.phi of implicit_diffusion). */
+int pearl_gpu_upload_trial_phi(pearl_gpu_ctx* ctx, const double* phi_aos3);
+/* implicit_diffusion (pearl_serial.cpp:1010-1094) on the trial phi; writes trial carbon and mu. */
+int pearl_gpu_implicit_diffusion(pearl_gpu_ctx* ctx, double dt, int* ok, int* iterations, double* residual,
+                                 double* closure);
+int pearl_gpu_download_trial(pearl_gpu_ctx* ctx, double* phi_aos3, double* carbon, double* mu);
+/* reduced_energy and total_carbon (pearl_serial.cpp:793-821, :784-788) of the current state. */
+int pearl_gpu_energy_mass(pearl_gpu_ctx* ctx, double* energy, double* mass);
+/* valid_state (pearl_serial.cpp:1096-1116) of the current state. */
+int pearl_gpu_valid_state(pearl_gpu_ctx* ctx, int* valid);
+
+/* ---- errors and accounting ---- */
+const char* pearl_gpu_status_string(int status);
+/* Message of the last failed call on this context (reference wording where one exists). */
+const char* pearl_gpu_last_error(const pearl_gpu_ctx* ctx);
+/* Device kernels launched by this context since creation; the grid size of the
+ * persistent kernel; the device time of the last launch in milliseconds. */
+int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* kernel_launches, int* grid_blocks, double* last_kernel_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PEARL_GPU_H */
