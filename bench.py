@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the Pearl FP64 time-step hot path on B200.
+
+Workload (the large FP64 configuration): nx=2048 periodic x 4096 growth rows,
+dx=2 nm, 64 lamellar pairs (spacing 32 cells with seeded +-10% jitter, ferrite
+fraction 0.875), per-column fronts at row 32+U{-1,0,1}, 20 K undercooling,
+adaptive dt (dt=4e-12 s, dt_max=8e-12 s), moving window enabled, implicit
+diffusion on.  Synthetic, seeded data; the 336 MB state is larger than L2.
+
+One step = one accepted pearl::advance (pearl_serial.cpp:1119) of the whole
+domain, including rejected attempts.  Metric: cell-updates/s = nx*ny*steps/time.
+
+  value    device-resident throughput: K steps in one persistent launch
+           (pearl_gpu_run), CUDA events on the launching stream.
+  e2e      the same through the public C ABI with host buffers: every output
+           interval uploads the state from pinned host memory, runs, applies
+           the moving window, reduces the diagnostics and downloads the state.
+  roofline algorithmic bytes per cell-update 80 + 64*n_CG (read+write of the
+           5-double state, plus per CG iteration read p,K,chi,x,r and write
+           x,r,p) over the kernel's event time, against the measured HBM copy
+           bandwidth.
+  cpu_baseline / --impl reference: the reference solver compiled from its own
+           source (oracle/_ref), else the C restatement, on host cores.
+
+Multi-GPU: the path does not shard (one resident domain per GPU), so N GPUs run
+N independent replicas ("scaling": "weak"); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "fe-c_eutectoid_phase-field_simulation_b200"
+for _p in (str(ROOT), str(PKG)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "cell-updates/s"
+UNIT = "cell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["pearl_gpu", "reference"], default="pearl_gpu")
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--ny", type=int, default=4096)
+    ap.add_argument("--output-every", type=int, default=50, help="accepted steps per e2e output interval")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bound of the CPU-baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=60.0, help="bound of the reference arm's timed work")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+def workload(nx: int, ny: int, seed: int = 0):
+    from pearl_gpu import workloads
+
+    return workloads.plain_large(seed=seed, nx=nx, ny=ny, pairs=max(1, nx // 32))
+
+
+def config_dict(w, args) -> dict:
+    return {
+        "workload": f"plain FP64 large: {w.nx}x{w.ny} (x periodic, y growth), 64 pairs spacing 32+-10%, "
+                    f"f_alpha 0.875, T_E-20K, adaptive dt, moving window, implicit diffusion",
+        "nx": w.nx, "ny": w.ny, "cells": w.cells, "dx_m": w.params["dx"],
+        "dt": w.params["dt_max"] / 2, "dt_max": w.params["dt_max"],
+        "l2": "inputs larger than L2 (state 40 B/cell = %.0f MB)" % (40 * w.cells / 1e6),
+        "parallelism": f"replicas x{args.gpus}",
+        "bytes_per_cell_update": "80 + 64*n_CG",
+    }
+
+
+# ------------------------------------------------------------------ helpers
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:  # noqa: BLE001
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_cell():
+    """DRAM bytes per cell-update of pearl_kernel from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / "pearl_kernel_fp64_plain_large.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_cell_update:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"pearl_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower().startswith("active")})
+        sm = [s for s, _, _ in rows]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(m for _, m, _ in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU sides
+def cpu_sample(w, seconds: float, max_steps: int | None = None):
+    """Time the reference (or the C restatement) on one host core over whole steps of the
+    same workload, stopping once `seconds` have elapsed.  Returns (rate, kind, steps, secs)."""
+    from oracle import pyoracle
+
+    ref = pyoracle.reference()
+    lib, kind = (ref, "reference") if ref is not None else (pyoracle.port(), "port")
+    phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    s = pyoracle.scalars_from(w.scalars)
+    steps, t_total = 0, 0.0
+    while t_total < seconds and (max_steps is None or steps < max_steps):
+        t0 = time.perf_counter()
+        out = lib.advance_n(w.params, phi, c, mu, s, 1)
+        t_total += time.perf_counter() - t0
+        if out[0] != 0:
+            raise RuntimeError(f"CPU baseline failed: {out[1]}")
+        steps += 1
+    return w.cells * steps / t_total, kind, steps, t_total
+
+
+def reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    w = workload(args.nx, args.ny)
+    from oracle import pyoracle
+
+    ref = pyoracle.reference()
+    lib, kind = (ref, "reference") if ref is not None else (pyoracle.port(), "port")
+    # Bounded: one whole warm-up step, then whole steps until --ref-seconds of
+    # timed work (about 14 s per step of the full domain on one core) or K steps.
+    warm = min(args.warmup, 1)
+    phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    s = pyoracle.scalars_from(w.scalars)
+    rc = lib.advance_n(w.params, phi, c, mu, s, warm)
+    if rc[0]:
+        raise RuntimeError(rc[1])
+    timed, dt = 0, 0.0
+    while timed < args.steps and (timed == 0 or dt < args.ref_seconds):
+        t0 = time.perf_counter()
+        rc = lib.advance_n(w.params, phi, c, mu, s, 1)
+        dt += time.perf_counter() - t0
+        if rc[0]:
+            raise RuntimeError(rc[1])
+        timed += 1
+    value = w.cells * timed / dt
+    sample = (f"{timed} timed whole steps after {warm} warm-up step of the full {w.nx}x{w.ny} workload "
+              f"(requested {args.steps}+{args.warmup}; bounded to about {args.ref_seconds:.0f} s)")
+    cores = 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": timed, "warmup": warm,
+        "ms_per_step": dt / timed * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": config_dict(w, args), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+                         "cpu": _cpu_model()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------ GPU arm
+def gpu_arm(args, rank: int, world: int, dist) -> None:
+    import numpy as np
+    import torch
+
+    import pearl_gpu
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    w = workload(args.nx, args.ny, seed=rank)
+    ctx = pearl_gpu.Context(w.params, w.nx, w.ny, device=local, stream=stream.cuda_stream)
+    # pinned host buffers for the end-to-end leg
+    phi_h = torch.from_numpy(w.phi).pin_memory().numpy()
+    c_h = torch.from_numpy(w.carbon).pin_memory().numpy()
+    mu_h = torch.from_numpy(w.mu).pin_memory().numpy()
+    ctx.upload(phi_h, c_h, mu_h, w.scalars)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # warm-up (also fills the step-energy cache)
+    ctx.run(max(args.warmup, 1))
+    meta = w.meta
+
+    # ---- device-resident timed region: K accepted steps in one persistent launch
+    clocks = ClockSampler(local)
+    barrier()
+    launches0 = ctx.stats()["launches"]
+    rejected0 = ctx.scalars().rejected
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    rep = ctx.run(args.steps)
+    ev1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    launches = ctx.stats()["launches"] - launches0
+    kernel_ms = ctx.stats()["last_ms"]
+    phase_ms = {k: round(v[0], 3) for k, v in ctx.phase_times().items()}
+    phase_n = {k: v[1] for k, v in ctx.phase_times().items()}
+    rejected = ctx.scalars().rejected - rejected0
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    assert rep.steps == args.steps, "run stopped early"
+    t_max = max_over_ranks(elapsed)
+    cells_total = sum_over_ranks(float(w.cells * rep.steps))
+    value = cells_total / t_max
+
+    # roofline of the persistent kernel: algorithmic bytes of its launch over its event time
+    algo_bytes = w.cells * (80.0 * rep.steps + 64.0 * rep.cg_total)
+    achieved = algo_bytes / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    tpc = ncu_traffic_per_cell()
+    traffic = tpc * w.cells * rep.steps if tpc is not None else None
+
+    # ---- end-to-end through the C ABI with host buffers
+    m = max(1, min(args.output_every, args.steps))
+    intervals = max(1, math.ceil(args.steps / m))
+    phi_o = torch.empty(w.phi.shape, dtype=torch.float64).pin_memory().numpy()
+    c_o = torch.empty(w.carbon.shape, dtype=torch.float64).pin_memory().numpy()
+    mu_o = torch.empty(w.mu.shape, dtype=torch.float64).pin_memory().numpy()
+    phi_h[...], c_h[...], mu_h[...], s_h = ctx.download()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = 0
+    for _ in range(intervals):
+        ctx.upload(phi_h, c_h, mu_h, s_h)
+        r = ctx.run(m)
+        e2e_steps += r.steps
+        ctx.maybe_shift(meta["shift_trigger"], meta["shift_target"], meta["shift_gamma_carbon"])
+        ctx.snapshot()
+        phi_o[...], c_o[...], mu_o[...], s_h = ctx.download()
+        phi_h, phi_o = phi_o, phi_h
+        c_h, c_o = c_o, c_h
+        mu_h, mu_o = mu_o, mu_h
+    barrier()
+    e2e_t = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = sum_over_ranks(float(w.cells * e2e_steps)) / e2e_t
+    bytes_state = 40 * w.cells
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, steps, secs = cpu_sample(w, args.cpu_seconds)
+        cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"{steps} whole steps of the same {w.nx}x{w.ny} workload in {secs:.1f} s "
+                         f"(single-threaded serial solver)", "cpu": _cpu_model()}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(w, args),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth",
+                         "kernel": "pearl_kernel (persistent FP64 step)",
+                         "algorithmic_bytes_per_launch": algo_bytes, "cg_iterations": rep.cg_total,
+                         "rejected_attempts": rejected, "phase_ms": phase_ms, "phase_count": phase_n},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state,
+                    "d2h_bytes_per_step": bytes_state,
+                    "step": f"one output interval of {m} accepted steps: upload state, run, maybe_shift, "
+                            f"snapshot, download state"},
+            "clocks": clock_info,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        backend = "nccl" if args.impl == "pearl_gpu" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world)
+        else:
+            gpu_arm(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -76,6 +76,15 @@ struct Ctl {
     int cg_peak, reached_stop;
     double out[8];
     int iout[4];
+    // per-phase device time of the last launch, measured by block 0 between
+    // consecutive grid barriers (phase compute + reduction + barrier wait)
+    unsigned long long phase_ns[16];
+    unsigned long long phase_count[16];
+};
+
+enum PhaseTag : int {
+    kTagPropose = 0, kTagSetup, kTagApply, kTagUpdate, kTagTrueRes, kTagReset, kTagFinal, kTagEnergy,
+    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagCount
 };
 
 // ---------------------------------------------------------------- thermodynamics

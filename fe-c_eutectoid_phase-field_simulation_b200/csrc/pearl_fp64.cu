@@ -160,19 +160,47 @@ __device__ __forceinline__ bool bad_cell(const DevParams& P, double q0, double q
 }
 
 // ------------------------------------------------------------------ the kernel
+struct PhaseClock {
+    unsigned long long t_last;
+    unsigned long long ns[kTagCount];
+    unsigned cnt[kTagCount];
+};
+
 struct Red {
     const KArgs& a;
+    PhaseClock* clk;  // shared memory; used by thread 0 of block 0 only
     unsigned counter = 0;
-    __device__ explicit Red(const KArgs& args) : a(args) {}
+    __device__ Red(const KArgs& args, PhaseClock* c) : a(args), clk(c) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            clk->t_last = globaltimer_ns();
+            for (int k = 0; k < kTagCount; ++k) {
+                clk->ns[k] = 0;
+                clk->cnt[k] = 0;
+            }
+        }
+    }
     // publish the block partials, wait for the grid, combine; false on a device-wait timeout
     template <int NV>
-    __device__ bool reduce(double (&v)[NV], unsigned ops) {
+    __device__ bool reduce(double (&v)[NV], unsigned ops, int tag) {
         double* slot = a.B.part + (size_t)(counter & 1u) * gridDim.x * kMaxRed;
         ++counter;
         block_publish<NV>(v, ops, slot);
         if (!grid_barrier(a.B.ctl, gridDim.x)) return false;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long t = globaltimer_ns();
+            clk->ns[tag] += t - clk->t_last;
+            clk->cnt[tag] += 1;
+            clk->t_last = t;
+        }
         grid_gather<NV>(v, ops, slot);
         return true;
+    }
+    __device__ void flush() const {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            for (int k = 0; k < kTagCount; ++k) {
+                a.B.ctl->phase_ns[k] = clk->ns[k];
+                a.B.ctl->phase_count[k] = clk->cnt[k];
+            }
     }
 };
 
@@ -255,7 +283,7 @@ __device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, doub
         }
     }
     double v[3] = {vchange, vmix, vsimp};
-    if (!red.reduce<3>(v, OPS3(kMax, kMax, kMax))) return false;
+    if (!red.reduce<3>(v, OPS3(kMax, kMax, kMax), kTagPropose)) return false;
     change = v[0];
     mixbad = v[1] != 0;
     simplexbad = v[2] != 0;
@@ -278,7 +306,7 @@ __device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
         B.icpt[c.i] = fma(chi, P.mu_ref, cint);
     }
     double v[1] = {vmix};
-    if (!red.reduce<1>(v, kMax)) return false;
+    if (!red.reduce<1>(v, kMax, kTagMix)) return false;
     mixbad = v[0] != 0;
     return true;
 }
@@ -312,7 +340,7 @@ __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double
         s2 += r * r;
     }
     double v[3] = {s0, s1, s2};
-    if (!red.reduce<3>(v, OPS3(kSum, kSum, kSum))) return false;
+    if (!red.reduce<3>(v, OPS3(kSum, kSum, kSum), kTagSetup)) return false;
     rhs2 = v[0];
     rz = v[1];
     rr = v[2];
@@ -351,7 +379,7 @@ __device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, dou
         s += pc * Ap;
     }
     double v[1] = {s};
-    if (!red.reduce<1>(v, kSum)) return false;
+    if (!red.reduce<1>(v, kSum, kTagApply)) return false;
     pAp = v[0];
     return true;
 }
@@ -375,7 +403,7 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
         s1 += r * r;
     }
     double v[2] = {s0, s1};
-    if (!red.reduce<2>(v, OPS2(kSum, kSum))) return false;
+    if (!red.reduce<2>(v, OPS2(kSum, kSum), kTagUpdate)) return false;
     rz = v[0];
     rr = v[1];
     return true;
@@ -397,7 +425,7 @@ __device__ bool phase_true_residual(const KArgs& a, Red& red, int cur, double dt
         s += r * r;
     }
     double v[1] = {s};
-    if (!red.reduce<1>(v, kSum)) return false;
+    if (!red.reduce<1>(v, kSum, kTagTrueRes)) return false;
     rr = v[0];
     return true;
 }
@@ -416,7 +444,7 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
         s += r * z;
     }
     double v[1] = {s};
-    if (!red.reduce<1>(v, kSum)) return false;
+    if (!red.reduce<1>(v, kSum, kTagReset)) return false;
     rz = v[0];
     return true;
 }
@@ -451,7 +479,7 @@ __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double
         ven += energy_cell(P, c, q0, q1, q2, tp, cn, chi, icpt);
     }
     double v[4] = {vclos, vbad, vmass, ven};
-    if (!red.reduce<4>(v, OPS4(kMax, kMax, kSum, kSum))) return false;
+    if (!red.reduce<4>(v, OPS4(kMax, kMax, kSum, kSum), kTagFinal)) return false;
     closure = v[0];
     bad = v[1] != 0;
     mass = v[2] * P.dx * P.dy;
@@ -475,7 +503,7 @@ __device__ bool phase_final_phase_only(const KArgs& a, Red& red, int cur, bool& 
         ven += energy_cell(P, c, q0, q1, q2, tp, 0.0, B.chi[c.i], B.icpt[c.i]);
     }
     double v[2] = {vbad, ven};
-    if (!red.reduce<2>(v, OPS2(kMax, kSum))) return false;
+    if (!red.reduce<2>(v, OPS2(kMax, kSum), kTagFinalPhaseOnly)) return false;
     bad = v[0] != 0;
     energy = v[1] * P.dx * P.dy;
     return true;
@@ -504,7 +532,7 @@ __device__ bool phase_energy(const KArgs& a, Red& red, int s, double& energy, do
         if (bad_cell(P, q0, q1, q2, cc, B.mu[s][c.i])) vbad = 1;
     }
     double v[4] = {ven, vmass, vmix, vbad};
-    if (!red.reduce<4>(v, OPS4(kSum, kSum, kMax, kMax))) return false;
+    if (!red.reduce<4>(v, OPS4(kSum, kSum, kMax, kMax), kTagEnergy)) return false;
     energy = v[0] * P.dx * P.dy;
     mass = v[1] * P.dx * P.dy;
     mixbad = v[2] != 0;
@@ -696,7 +724,7 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
         if (av >= 0 && bv < 0) local = fmax(local, ((c.y + 1) - .5 + av / (av - bv)) * P.dy);
     }
     double v1[1] = {local};
-    if (!red.reduce<1>(v1, kMax)) return false;
+    if (!red.reduce<1>(v1, kMax, kTagShift)) return false;
     const double front = v1[0];
     if (blockIdx.x == 0 && threadIdx.x == 0) a.B.ctl->out[0] = front;
     if (front < a.shift_trigger) return true;
@@ -708,7 +736,7 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
         gmax = fmax(gmax, g[c.i]);
     }
     double v2[1] = {gmax};
-    if (!red.reduce<1>(v2, kMax)) return false;
+    if (!red.reduce<1>(v2, kMax, kTagShift)) return false;
     if (v2[0] > 1e-6) {
         set_error(B.ctl, PEARL_ERR_UNSAFE_SHIFT, 0);
         return false;
@@ -746,7 +774,7 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
         B.mu[nw][c.i] = (cc - cint) / chi;  // close_mu / reconstruct_mu (:139-142, :789-792)
     }
     double v3[3] = {removed, vmix, vnonfin};
-    if (!red.reduce<3>(v3, OPS3(kSum, kMax, kMax))) return false;
+    if (!red.reduce<3>(v3, OPS3(kSum, kMax, kMax), kTagShift)) return false;
     if (v3[1] != 0) {
         set_error(B.ctl, PEARL_ERR_MIXTURE, 0);
         return false;
@@ -783,14 +811,15 @@ __device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
         sumerr = fmax(sumerr, fabs(ph[0][c.i] + ph[1][c.i] + ph[2][c.i] - 1));
     }
     double v[5] = {minc, maxc, minmu, maxmu, sumerr};
-    if (!red.reduce<5>(v, OPS5(kMin, kMax, kMin, kMax, kMax))) return false;
+    if (!red.reduce<5>(v, OPS5(kMin, kMax, kMin, kMax, kMax), kTagSnapshot)) return false;
     for (int k = 0; k < 5; ++k) out[k] = v[k];
     return true;
 }
 
 __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs a) {
     Ctl* ctl = a.B.ctl;
-    Red red(a);
+    __shared__ PhaseClock clk;
+    Red red(a, &clk);
     StepState st;
     st.S = ctl->S;
     st.cur = ctl->cur;
@@ -833,6 +862,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->reached_stop = reached;
             ctl->last = last;
         }
+        red.flush();
         return;
     }
     if (a.mode == kModePropose) {
@@ -844,12 +874,14 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->iout[0] = mixbad;
             ctl->iout[1] = simplexbad;
         }
+        red.flush();
         return;
     }
     if (a.mode == kModeMix) {
         bool mixbad;
         if (!phase_mix(a, red, st.cur, mixbad)) return;
         if (leader) ctl->iout[0] = mixbad;
+        red.flush();
         return;
     }
     if (a.mode == kModeDiffusion) {
@@ -861,6 +893,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->out[0] = d.residual;
             ctl->out[1] = d.closure;
         }
+        red.flush();
         return;
     }
     if (a.mode == kModeEnergy || a.mode == kModeValid) {
@@ -873,6 +906,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->iout[0] = mixbad;
             ctl->iout[1] = bad;
         }
+        red.flush();
         return;
     }
     if (a.mode == kModeSnapshot) {
@@ -887,6 +921,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->out[6] = e;
             ctl->iout[0] = mixbad;
         }
+        red.flush();
         return;
     }
     if (a.mode == kModeMaybeShift) {
@@ -898,6 +933,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->energy_valid = st.cache_valid ? 1 : 0;
             ctl->iout[0] = rows;
         }
+        red.flush();
         return;
     }
 }
@@ -1431,6 +1467,15 @@ int pearl_gpu_valid_state(pearl_gpu_ctx* ctx, int* valid) {
     int rc = launch(ctx, a);
     if (rc) return rc;
     *valid = ctx->h_ctl->iout[1] ? 0 : 1;
+    return PEARL_OK;
+}
+
+int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 16; ++k) {
+        if (ms) ms[k] = k < kTagCount ? ctx->h_ctl->phase_ns[k] * 1e-6 : 0.0;
+        if (counts) counts[k] = k < kTagCount ? (long long)ctx->h_ctl->phase_count[k] : 0;
+    }
     return PEARL_OK;
 }
 

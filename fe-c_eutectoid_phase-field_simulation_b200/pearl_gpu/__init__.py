@@ -106,8 +106,11 @@ EXPORTS = [
     "pearl_gpu_download", "pearl_gpu_get_scalars", "pearl_gpu_set_scalars", "pearl_gpu_advance", "pearl_gpu_run",
     "pearl_gpu_maybe_shift", "pearl_gpu_snapshot", "pearl_gpu_propose_phi", "pearl_gpu_upload_trial_phi",
     "pearl_gpu_implicit_diffusion", "pearl_gpu_download_trial", "pearl_gpu_energy_mass", "pearl_gpu_valid_state",
-    "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats",
+    "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats", "pearl_gpu_phase_times",
 ]
+
+PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
+          "mixture", "shift", "snapshot"]
 
 _lib = None
 
@@ -146,6 +149,7 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_last_error.argtypes = [V]
     L.pearl_gpu_last_error.restype = C.c_char_p
     L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
+    L.pearl_gpu_phase_times.argtypes = [V, DP, C.POINTER(C.c_longlong)]
     if path is None:
         _lib = L
     return L
@@ -279,6 +283,13 @@ class Context:
         v = C.c_int()
         self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
         return bool(v.value)
+
+    def phase_times(self) -> dict:
+        """{phase: (ms, count)} of the last launch."""
+        ms = (D * 16)()
+        cnt = (C.c_longlong * 16)()
+        self._check(self.lib.pearl_gpu_phase_times(self.h, ms, cnt))
+        return {name: (ms[k], cnt[k]) for k, name in enumerate(PHASES) if cnt[k]}
 
     def stats(self):
         n, g, ms = C.c_longlong(), C.c_int(), D()

@@ -8,8 +8,10 @@ direction) has zero-flux walls and the transformation front moves towards +y
 
 Geometry of every workload: lamellar pairs of ferrite (alpha) and cementite
 (theta) columns fill the rows below a front; austenite (gamma) fills the rest.
-Interfaces are tanh profiles ``0.5*(1 - tanh(d/delta))`` with ``delta`` = 1
-cell, i.e. about 4 cells from 2% to 98%.  Phase fractions are built like the
+Interfaces are tanh profiles ``0.5*(1 - tanh(d/delta))`` with ``delta`` = 2
+cells: 4 cells wide between 12% and 88% (the tanh width 2*delta).  A 1-cell
+delta with the +-1-row front jitter is sharper than the model can relax: the
+reference itself then shrinks dt below dt_min within ~35 steps.  Phase fractions are built like the
 reference's ``lamella`` initialisation (pearl_serial.cpp:1768-1770):
 ``phi = ((1-Theta)*P, Theta*P, 1-P)``.  The chemical potential starts uniform
 at the eutectoid austenite composition and carbon is ``c = chi*mu + c0`` per
@@ -136,7 +138,7 @@ def _mixture(phi: np.ndarray, params: dict):
     return chi, c0
 
 
-def lamellar_phi(nx: int, ny: int, widths, theta_widths, front_rows, delta: float = 1.0) -> np.ndarray:
+def lamellar_phi(nx: int, ny: int, widths, theta_widths, front_rows, delta: float = 2.0) -> np.ndarray:
     """phi[ny, nx, 3] for lamellar pairs (theta first in each pair) below per-column fronts."""
     widths = np.asarray(widths, dtype=np.int64)
     assert int(widths.sum()) == nx

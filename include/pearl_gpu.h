@@ -175,6 +175,12 @@ const char* pearl_gpu_last_error(const pearl_gpu_ctx* ctx);
 /* Device kernels launched by this context since creation; the grid size of the
  * persistent kernel; the device time of the last launch in milliseconds. */
 int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* kernel_launches, int* grid_blocks, double* last_kernel_ms);
+/* Device time of the last launch split by phase (16 slots, milliseconds and
+ * phase counts): 0 propose, 1 diffusion set-up, 2 CG apply, 3 CG update,
+ * 4 true residual, 5 CG restart, 6 diffusion final + acceptance reductions,
+ * 7 step-start energy, 8 phase-only final, 9 mixture, 10 moving window,
+ * 11 snapshot.  Each slot covers its sweep, reduction and grid barrier. */
+int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts);
 
 #ifdef __cplusplus
 }

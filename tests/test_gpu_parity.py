@@ -60,7 +60,9 @@ def test_implicit_diffusion(gpu_lib, port, nx, ny, front):
     rc, c_o, mu_o, info = port.implicit_diffusion(w.params, w.carbon, w.mu, trial_phi, dt)
     assert rc == 0 and info.ok == 1 and d["ok"] == 1
     assert d["it"] == info.it
-    assert abs(d["residual"] - info.residual) <= 1e-6 * info.residual + 1e-30
+    # the converged true residual is a norm of rounding-level values (~1e-16):
+    # different dot-product orders move it in the 5th digit
+    assert abs(d["residual"] - info.residual) <= 1e-3 * info.residual + 1e-30
     assert np.abs(mu_g - mu_o).max() <= MU_TOL
     assert np.abs(c_g - c_o).max() <= 1e-14
     assert abs(c_g.sum() - c_o.sum()) <= MASS_RTOL * abs(c_o.sum())
