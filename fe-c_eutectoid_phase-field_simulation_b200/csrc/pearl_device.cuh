@@ -16,8 +16,9 @@
 
 namespace pearl_gpu {
 
-constexpr int kTileX = 32;  // one warp spans 32 consecutive x cells (256 B of a row)
-constexpr int kTileY = 8;   // 8 warps stack 8 rows
+constexpr int kTileX = 32;     // one warp spans 32 consecutive x cells (256 B of a row)
+constexpr int kTileY = 8;      // 8 warps per block
+constexpr int kTileRows = 16;  // each warp covers two adjacent rows
 constexpr int kThreads = kTileX * kTileY;
 constexpr int kMaxRed = 6;  // values per grid reduction
 
@@ -39,7 +40,31 @@ struct DevParams {
     double mass_scale;    // gx*gy*dx*dy*1e-6                  (:1152)
     double energy_scale;  // sigma*max(gx*dx, gy*dy)            (:1157)
     int cg_max, max_retries, check_energy, phase_only;
+    // RN(1/b) of every constant divisor b, for div_by
+    double r_Vm, r_dx, r_dy, r_dx2, r_dy2, r_3, r_two_A[3];
+    int exact_div;  // 1 when every constant divisor and its reciprocal are normal numbers
 };
+
+// a/b, correctly rounded, for a divisor b whose reciprocal rb = RN(1/b) was
+// computed once on the host.  Residual correction with fused multiply-adds
+// (Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et al., Handbook of
+// Floating-Point Arithmetic, ch. "Division"): q0 = a*rb, then twice
+// q <- q + (a - q*b)*rb, where a - q*b is exact in one FMA.  After the first
+// correction q is a faithful quotient, and Markstein's theorem makes the
+// second one the correctly rounded a/b for normal operands and quotients, so
+// the result equals IEEE division bitwise (checked on the device against
+// '/' by pearl_gpu_selftest_division).  Zero and non-finite numerators keep
+// the sign/special value of a*rb.  Falls back to '/' when the host found a
+// divisor outside the normal range.
+__device__ __forceinline__ double div_by(const DevParams& P, double a, double b, double rb) {
+    if (!P.exact_div) return a / b;
+    const double q0 = a * rb;
+    double r = fma(-q0, b, a);
+    double q = fma(r, rb, q0);
+    r = fma(-q, b, a);
+    q = fma(r, rb, q);
+    return (a == 0.0 || !isfinite(q0)) ? q0 : q;
+}
 
 // Device buffers: two state sets (current / trial, selected by Ctl::cur) and
 // the work vectors of the implicit solve.  Every plane is ny rows of `pitch`
@@ -119,7 +144,9 @@ __device__ __forceinline__ bool mixture(const DevParams& P, double p0, double p1
 
 // project_simplex (pearl_serial.cpp:491-509).  Inputs are finite here (the
 // caller checks first, :990-996).  Returns false where the reference throws.
-__device__ __forceinline__ bool project_simplex(double& z0, double& z1, double& z2) {
+// The thresholds (sum-1)/1, /2, /3 are formed exactly: x/1 = x, x/2 = x*0.5,
+// and /3 through div_by.
+__device__ __forceinline__ bool project_simplex(const DevParams& P, double& z0, double& z1, double& z2) {
     double s0 = z0, s1 = z1, s2 = z2, t;
     if (s0 < s1) { t = s0; s0 = s1; s1 = t; }
     if (s1 < s2) { t = s1; s1 = s2; s2 = t; }
@@ -127,13 +154,13 @@ __device__ __forceinline__ bool project_simplex(double& z0, double& z1, double& 
     double sum = 0.0, threshold = 0.0, cand;
     int active = 0;
     sum += s0;
-    cand = (sum - 1.0) / 1;
+    cand = sum - 1.0;
     if (s0 > cand) { active = 1; threshold = cand; }
     sum += s1;
-    cand = (sum - 1.0) / 2;
+    cand = (sum - 1.0) * 0.5;
     if (s1 > cand) { active = 2; threshold = cand; }
     sum += s2;
-    cand = (sum - 1.0) / 3;
+    cand = div_by(P, sum - 1.0, 3.0, P.r_3);
     if (s2 > cand) { active = 3; threshold = cand; }
     // std::max(0.0, v) == (0.0 < v ? v : 0.0)
     double v = z0 - threshold;

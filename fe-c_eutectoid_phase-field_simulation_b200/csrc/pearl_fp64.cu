@@ -3,7 +3,7 @@
 // including the retry loop and the Jacobi-PCG solve, with every decision
 // (dt, acceptance, CG termination) taken on the device.
 //
-// Phases of one attempt (each is a sweep over 32x8-cell tiles followed by a
+// Phases of one attempt (each is a sweep over 32x16-cell tiles followed by a
 // deterministic grid reduction and a bounded grid barrier):
 //   PROPOSE  propose_phi (:961-1002) + mixture of the trial phi (:1013-1020)
 //   SETUP    implicit_diffusion set-up: apply(mu_offset), r, z, diag (:1021-1046)
@@ -13,6 +13,11 @@
 //   RESET    z = r/diag ; <r,z>                                      (:1060-1064)
 //   FINAL    conservative carbon update, closure, mu, valid_state,
 //            total_carbon and reduced_energy of the trial state      (:1082-1093, :1096-1116, :784-821)
+//
+// Thread mapping: a warp covers 32 consecutive x of two adjacent rows; the
+// eight warps of a block stack 16 rows.  The two cells of a thread share their
+// vertical neighbour loads, and every load of a streaming phase is issued
+// before its arithmetic, doubling the bytes in flight per thread.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,43 +53,88 @@ struct KArgs {
     double shift_trigger, shift_target, shift_c_gamma;
 };
 
-struct Cell {
-    int x, y;
-    size_t i, iw, ie, is, in;
-    bool ok;
+// The two cells (x, y0) and (x, y0+1) of one thread in tile t.
+struct Pair {
+    int x, y0;
+    bool v0, v1;                   // cell valid (inside the domain)
+    size_t i0, i1;                 // centres
+    size_t iw0, ie0, iw1, ie1;     // x neighbours (periodic)
+    size_t is0, in1;               // y neighbours outside the pair (zero-flux ghost = the cell itself)
 };
 
-__device__ __forceinline__ Cell cell_of(const DevParams& P, int t) {
-    Cell c;
+__device__ __forceinline__ Pair pair_of(const DevParams& P, int t) {
+    Pair c;
     const int bx = t % P.ntx, by = t / P.ntx;
     c.x = bx * kTileX + (threadIdx.x & 31);
-    c.y = by * kTileY + (threadIdx.x >> 5);
-    c.ok = c.x < P.nx && c.y < P.ny;
+    c.y0 = by * kTileRows + 2 * (threadIdx.x >> 5);
+    c.v0 = c.x < P.nx && c.y0 < P.ny;
+    c.v1 = c.v0 && c.y0 + 1 < P.ny;
     const int xw = c.x == 0 ? P.nx - 1 : c.x - 1;
     const int xe = c.x == P.nx - 1 ? 0 : c.x + 1;
-    const size_t row = (size_t)c.y * P.pitch;
-    c.i = row + c.x;
-    c.iw = row + xw;
-    c.ie = row + xe;
-    // zero-flux ghosts copy the edge row (pearl_serial.cpp:690-691)
-    c.is = c.y > 0 ? c.i - P.pitch : c.i;
-    c.in = c.y < P.ny - 1 ? c.i + P.pitch : c.i;
+    const size_t row = (size_t)c.y0 * P.pitch;
+    c.i0 = row + c.x;
+    c.i1 = c.i0 + P.pitch;
+    c.iw0 = row + xw;
+    c.ie0 = row + xe;
+    c.iw1 = c.iw0 + P.pitch;
+    c.ie1 = c.ie0 + P.pitch;
+    c.is0 = c.y0 > 0 ? c.i0 - P.pitch : c.i0;
+    c.in1 = c.y0 + 2 < P.ny ? c.i1 + P.pitch : c.i1;
     return c;
+}
+
+// Five-point stencils of one field for both cells of a pair.  For the cell
+// below, the north value is the upper cell; for the upper cell, the south value
+// is the lower cell.  When the upper cell is outside the domain the lower cell
+// is the top row and its north ghost is itself.
+struct S2 {
+    double c0, c1, w0, e0, w1, e1, s0, n1;
+};
+__device__ __forceinline__ S2 load_s2(const double* f, const Pair& c) {
+    S2 s;
+    s.c0 = f[c.i0];
+    s.w0 = f[c.iw0];
+    s.e0 = f[c.ie0];
+    s.s0 = f[c.is0];
+    if (c.v1) {
+        s.c1 = f[c.i1];
+        s.w1 = f[c.iw1];
+        s.e1 = f[c.ie1];
+        s.n1 = f[c.in1];
+    } else {
+        s.c1 = s.c0;
+        s.w1 = s.e1 = s.n1 = 0;
+    }
+    return s;
 }
 
 // Face weights of implicit_diffusion's weights_at (pearl_serial.cpp:1022-1028)
 struct Faces {
     double w0, w1, w2, w3;
 };
-__device__ __forceinline__ Faces faces_at(const DevParams& P, const double* K, const Cell& c) {
-    const double k = K[c.i];
+__device__ __forceinline__ double face_x(const DevParams& P, double k, double kn) {
+    return div_by(P, .5 * (k + kn), P.dx2, P.r_dx2);
+}
+__device__ __forceinline__ double face_y(const DevParams& P, double k, double kn) {
+    return div_by(P, .5 * (k + kn), P.dy2, P.r_dy2);
+}
+__device__ __forceinline__ Faces faces0(const DevParams& P, const S2& K, const Pair& c) {
     Faces f;
-    f.w0 = .5 * (k + K[c.iw]) / P.dx2;
-    f.w1 = .5 * (k + K[c.ie]) / P.dx2;
-    f.w2 = .5 * (k + K[c.is]) / P.dy2;
-    f.w3 = .5 * (k + K[c.in]) / P.dy2;
-    if (c.y == 0) f.w2 = 0;
-    if (c.y == P.ny - 1) f.w3 = 0;
+    f.w0 = face_x(P, K.c0, K.w0);
+    f.w1 = face_x(P, K.c0, K.e0);
+    f.w2 = face_y(P, K.c0, K.s0);
+    f.w3 = face_y(P, K.c0, K.c1);
+    if (c.y0 == 0) f.w2 = 0;
+    if (c.y0 == P.ny - 1) f.w3 = 0;
+    return f;
+}
+__device__ __forceinline__ Faces faces1(const DevParams& P, const S2& K, const Pair& c) {
+    Faces f;
+    f.w0 = face_x(P, K.c1, K.w1);
+    f.w1 = face_x(P, K.c1, K.e1);
+    f.w2 = face_y(P, K.c1, K.c0);
+    f.w3 = face_y(P, K.c1, K.n1);
+    if (c.y0 + 1 == P.ny - 1) f.w3 = 0;
     return f;
 }
 
@@ -93,16 +143,30 @@ __device__ __forceinline__ double apply_at(double chi, double dt, const Faces& f
                                            double us, double un) {
     return chi * u + dt * (f.w0 * (u - uw) + f.w1 * (u - ue) + f.w2 * (u - us) + f.w3 * (u - un));
 }
+__device__ __forceinline__ double apply0(double chi, double dt, const Faces& f, const S2& u) {
+    return apply_at(chi, dt, f, u.c0, u.w0, u.e0, u.s0, u.c1);
+}
+__device__ __forceinline__ double apply1(double chi, double dt, const Faces& f, const S2& u) {
+    return apply_at(chi, dt, f, u.c1, u.w1, u.e1, u.c0, u.n1);
+}
+// conservative carbon change of the final update (pearl_serial.cpp:1085)
+__device__ __forceinline__ double flux_at(double dt, const Faces& f, double u, double uw, double ue, double us,
+                                          double un) {
+    return dt * (f.w0 * (uw - u) + f.w1 * (ue - u) + f.w2 * (us - u) + f.w3 * (un - u));
+}
 
-// Per-cell reduced-energy density of reduced_energy (pearl_serial.cpp:800-819),
-// without the final dx*dy.  chi/icpt are mixture(phi).susceptibility and
-// composition(mu_ref, mixture(phi)).
-__device__ __forceinline__ double energy_cell(const DevParams& P, const Cell& c, double q0, double q1, double q2,
-                                              const double* const* phi, double carbon, double chi, double icpt) {
-    const double triple = 2.0 * q0 * q1 * q2;
-    const double h0 = q0 * q0 * (3.0 - 2.0 * q0) + triple;
-    const double h1 = q1 * q1 * (3.0 - 2.0 * q1) + triple;
-    const double h2 = q2 * q2 * (3.0 - 2.0 * q2) + triple;
+// Per-cell reduced-energy density (pearl_serial.cpp:800-819) without the final
+// dx*dy: cell terms, then the +x face, then the +y face unless at the top wall.
+// chi/icpt are mixture(phi).susceptibility and composition(mu_ref, mixture(phi)).
+struct Phi3 {
+    double a, t, g;
+};
+__device__ __forceinline__ double energy_cell(const DevParams& P, const Phi3& q, const Phi3& e, const Phi3& n,
+                                              bool has_n, double carbon, double chi, double icpt) {
+    const double triple = 2.0 * q.a * q.t * q.g;
+    const double h0 = q.a * q.a * (3.0 - 2.0 * q.a) + triple;
+    const double h1 = q.t * q.t * (3.0 - 2.0 * q.t) + triple;
+    const double h2 = q.g * q.g * (3.0 - 2.0 * q.g) + triple;
     double chem = 0;
     chem += h0 * P.psi_t[0];
     chem += h1 * P.psi_t[1];
@@ -111,55 +175,52 @@ __device__ __forceinline__ double energy_cell(const DevParams& P, const Cell& c,
         const double dc = carbon - icpt;
         chem += .5 * dc * dc / chi;
     }
-    double t = chem / P.Vm + P.obs * (q0 * q1 + q0 * q2 + q1 * q2) + P.tr * q0 * q1 * q2;
-    {
-        const double n0 = phi[0][c.ie], n1 = phi[1][c.ie], n2 = phi[2][c.ie];
-        double z = (q0 * n1 - n0 * q1) / P.dx;
+    double t = div_by(P, chem, P.Vm, P.r_Vm) + P.obs * (q.a * q.t + q.a * q.g + q.t * q.g) + P.tr * q.a * q.t * q.g;
+    double z = div_by(P, q.a * e.t - e.a * q.t, P.dx, P.r_dx);
+    t += P.eps_sigma * z * z;
+    z = div_by(P, q.a * e.g - e.a * q.g, P.dx, P.r_dx);
+    t += P.eps_sigma * z * z;
+    z = div_by(P, q.t * e.g - e.t * q.g, P.dx, P.r_dx);
+    t += P.eps_sigma * z * z;
+    if (has_n) {
+        z = div_by(P, q.a * n.t - n.a * q.t, P.dy, P.r_dy);
         t += P.eps_sigma * z * z;
-        z = (q0 * n2 - n0 * q2) / P.dx;
+        z = div_by(P, q.a * n.g - n.a * q.g, P.dy, P.r_dy);
         t += P.eps_sigma * z * z;
-        z = (q1 * n2 - n1 * q2) / P.dx;
-        t += P.eps_sigma * z * z;
-    }
-    if (c.y != P.ny - 1) {
-        const double n0 = phi[0][c.in], n1 = phi[1][c.in], n2 = phi[2][c.in];
-        double z = (q0 * n1 - n0 * q1) / P.dy;
-        t += P.eps_sigma * z * z;
-        z = (q0 * n2 - n0 * q2) / P.dy;
-        t += P.eps_sigma * z * z;
-        z = (q1 * n2 - n1 * q2) / P.dy;
+        z = div_by(P, q.t * n.g - n.t * q.g, P.dy, P.r_dy);
         t += P.eps_sigma * z * z;
     }
     return t;
 }
 
 // valid_state per cell (pearl_serial.cpp:1099-1114); true if the cell is bad.
-__device__ __forceinline__ bool bad_cell(const DevParams& P, double q0, double q1, double q2, double carbon,
-                                         double mu) {
+__device__ __forceinline__ bool bad_cell(const DevParams& P, const Phi3& q, double carbon, double mu) {
     bool good = true;
     double sum = 0;
-    good = good && isfinite(q0) && q0 >= -1e-12 && q0 <= 1 + 1e-12;
-    sum += q0;
-    good = good && isfinite(q1) && q1 >= -1e-12 && q1 <= 1 + 1e-12;
-    sum += q1;
-    good = good && isfinite(q2) && q2 >= -1e-12 && q2 <= 1 + 1e-12;
-    sum += q2;
+    good = good && isfinite(q.a) && q.a >= -1e-12 && q.a <= 1 + 1e-12;
+    sum += q.a;
+    good = good && isfinite(q.t) && q.t >= -1e-12 && q.t <= 1 + 1e-12;
+    sum += q.t;
+    good = good && isfinite(q.g) && q.g >= -1e-12 && q.g <= 1 + 1e-12;
+    sum += q.g;
     good = good && fabs(sum - 1) < 1e-10;
     good = good && isfinite(mu) && isfinite(carbon);
     if (!P.phase_only) {
         good = good && carbon >= -1e-10 && carbon <= 1 + 1e-10;
-        const double q[3] = {q0, q1, q2};
+        const double qq[3] = {q.a, q.t, q.g};
 #pragma unroll
         for (int a = 0; a < 3; ++a)
-            if (q[a] > .01) {
-                const double ca = (mu - P.B[a]) / P.two_A[a];
+            if (qq[a] > .01) {
+                const double ca = div_by(P, mu - P.B[a], P.two_A[a], P.r_two_A[a]);
                 good = good && ca >= -1e-10 && ca <= 1 + 1e-10;
             }
     }
     return !good;
 }
 
-// ------------------------------------------------------------------ the kernel
+__device__ __forceinline__ Phi3 load_phi(const double* const* ph, size_t i) { return Phi3{ph[0][i], ph[1][i], ph[2][i]}; }
+
+// ------------------------------------------------------------------ grid reductions
 struct PhaseClock {
     unsigned long long t_last;
     unsigned long long ns[kTagCount];
@@ -209,6 +270,68 @@ struct Red {
 #define OPS4(a, b, c, d) (OPS3(a, b, c) | ((unsigned)(d) << 6))
 #define OPS5(a, b, c, d, e) (OPS4(a, b, c, d) | ((unsigned)(e) << 8))
 
+#define FOR_TILES(P) for (int t = blockIdx.x; t < (P).ntiles; t += gridDim.x)
+
+// ------------------------------------------------------------------ phases
+// propose_phi for one cell (pearl_serial.cpp:966-1001); returns the trial phi.
+struct Proposal {
+    double z0, z1, z2, change;
+    bool simplex_bad;
+};
+__device__ __forceinline__ Proposal propose_cell(const DevParams& P, const double* const* ph, double mu, double dt,
+                                                 size_t i, size_t iw, size_t ie, size_t is, size_t in, bool south,
+                                                 bool north) {
+    const double q0 = ph[0][i], q1 = ph[1][i], q2 = ph[2][i];
+    const double psi0 = psi(P, 2, mu);
+    const double ps[3] = {psi(P, 0, mu), psi(P, 1, mu), psi0};
+    const double q[3] = {q0, q1, q2};
+    const double dtr[3] = {2.0 * q1 * q2, 2.0 * q0 * q2, 2.0 * q0 * q1};
+    double f[3];
+#pragma unroll
+    for (int aa = 0; aa < 3; ++aa) {
+        const double qa1 = q[(aa + 1) % 3], qa2 = q[(aa + 2) % 3];
+        f[aa] = P.obs * (qa1 + qa2) + P.tr * qa1 * qa2;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const double dh = dtr[aa] + (b == aa ? 6.0 * q[b] * (1.0 - q[b]) : 0.0);
+            f[aa] += div_by(P, (ps[b] - psi0) * dh, P.Vm, P.r_Vm);
+        }
+    }
+    // four faces in the reference's order: -x, +x, -y (not at y=0), +y (not at the top)
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        if ((dir == 2 && !south) || (dir == 3 && !north)) continue;
+        const size_t j = dir == 0 ? iw : (dir == 1 ? ie : (dir == 2 ? is : in));
+        const double n[3] = {ph[0][j], ph[1][j], ph[2][j]};
+        const double d2 = dir < 2 ? P.dx2 : P.dy2, rd2 = dir < 2 ? P.r_dx2 : P.r_dy2;
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+            for (int b = aa + 1; b < 3; ++b) {
+                const double w = div_by(P, P.two_eps_sigma * (q[aa] * n[b] - n[aa] * q[b]), d2, rd2);
+                f[aa] += w * n[b];
+                f[b] -= w * n[aa];
+            }
+    }
+    const double mean = div_by(P, f[0] + f[1] + f[2], 3.0, P.r_3);
+    const double scale = dt / (local_tau(P, q0, q1, q2) * P.eps);
+    Proposal o;
+    o.z0 = q0 - scale * (f[0] - mean);
+    o.z1 = q1 - scale * (f[1] - mean);
+    o.z2 = q2 - scale * (f[2] - mean);
+    o.simplex_bad = false;
+    if (!(isfinite(o.z0) && isfinite(o.z1) && isfinite(o.z2))) {
+        o.change = INFINITY;
+        o.z0 = q0;
+        o.z1 = q1;
+        o.z2 = q2;
+    } else {
+        o.simplex_bad = !project_simplex(P, o.z0, o.z1, o.z2);
+        o.change = fmax(fmax(fabs(o.z0 - q0), fabs(o.z1 - q1)), fabs(o.z2 - q2));
+    }
+    return o;
+}
+
 // PROPOSE: propose_phi from state `cur` into state `1-cur`, then the mixture of
 // the trial phi (K, chi, icpt); in phase_only mode also the reconstructed
 // trial carbon and the copied trial mu (pearl_serial.cpp:1134-1136).
@@ -220,66 +343,33 @@ __device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, doub
     const double* const* ph = B.phi[cur];
     double* const* tp = B.phi[cur ^ 1];
     double vchange = 0, vmix = 0, vsimp = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const double q0 = ph[0][c.i], q1 = ph[1][c.i], q2 = ph[2][c.i];
-        const double mu = B.mu[cur][c.i];
-        const double psi0 = psi(P, 2, mu);
-        const double ps[3] = {psi(P, 0, mu), psi(P, 1, mu), psi0};
-        const double q[3] = {q0, q1, q2};
-        const double dtr[3] = {2.0 * q1 * q2, 2.0 * q0 * q2, 2.0 * q0 * q1};
-        double f[3];
-#pragma unroll
-        for (int aa = 0; aa < 3; ++aa) {
-            const double qa1 = q[(aa + 1) % 3], qa2 = q[(aa + 2) % 3];
-            f[aa] = P.obs * (qa1 + qa2) + P.tr * qa1 * qa2;
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const double dh = dtr[aa] + (b == aa ? 6.0 * q[b] * (1.0 - q[b]) : 0.0);
-                f[aa] += (ps[b] - psi0) * dh / P.Vm;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !c.v1) break;
+            const int y = c.y0 + k;
+            const size_t i = k ? c.i1 : c.i0;
+            const size_t iw = k ? c.iw1 : c.iw0, ie = k ? c.ie1 : c.ie0;
+            const size_t is = k ? c.i0 : c.is0, in = k ? c.in1 : c.i1;
+            const double mu = B.mu[cur][i];
+            const Proposal o = propose_cell(P, ph, mu, dt, i, iw, ie, is, in, y > 0, y < P.ny - 1);
+            if (o.change == INFINITY) vchange = INFINITY;
+            else vchange = fmax(vchange, o.change);
+            if (o.simplex_bad) vsimp = 1;
+            tp[0][i] = o.z0;
+            tp[1][i] = o.z1;
+            tp[2][i] = o.z2;
+            double chi, cint, K;
+            if (!mixture(P, o.z0, o.z1, o.z2, chi, cint, K)) vmix = 1;
+            B.K[i] = K;
+            B.chi[i] = chi;
+            B.icpt[i] = fma(chi, P.mu_ref, cint);
+            if (P.phase_only) {
+                B.c[cur ^ 1][i] = fma(chi, mu, cint);
+                B.mu[cur ^ 1][i] = mu;
             }
-        }
-        // four faces in the reference's order: -x, +x, -y (not at y=0), +y (not at top)
-#pragma unroll
-        for (int dir = 0; dir < 4; ++dir) {
-            if ((dir == 2 && c.y == 0) || (dir == 3 && c.y == P.ny - 1)) continue;
-            const size_t j = dir == 0 ? c.iw : (dir == 1 ? c.ie : (dir == 2 ? c.is : c.in));
-            const double n[3] = {ph[0][j], ph[1][j], ph[2][j]};
-            const double d2 = dir < 2 ? P.dx2 : P.dy2;
-#pragma unroll
-            for (int aa = 0; aa < 3; ++aa)
-#pragma unroll
-                for (int b = aa + 1; b < 3; ++b) {
-                    const double w = P.two_eps_sigma * (q[aa] * n[b] - n[aa] * q[b]) / d2;
-                    f[aa] += w * n[b];
-                    f[b] -= w * n[aa];
-                }
-        }
-        const double mean = (f[0] + f[1] + f[2]) / 3, scale = dt / (local_tau(P, q0, q1, q2) * P.eps);
-        double z0 = q0 - scale * (f[0] - mean), z1 = q1 - scale * (f[1] - mean), z2 = q2 - scale * (f[2] - mean);
-        if (!(isfinite(z0) && isfinite(z1) && isfinite(z2))) {
-            vchange = INFINITY;
-            z0 = q0;
-            z1 = q1;
-            z2 = q2;
-        } else {
-            if (!project_simplex(z0, z1, z2)) vsimp = 1;
-            vchange = fmax(vchange, fabs(z0 - q0));
-            vchange = fmax(vchange, fabs(z1 - q1));
-            vchange = fmax(vchange, fabs(z2 - q2));
-        }
-        tp[0][c.i] = z0;
-        tp[1][c.i] = z1;
-        tp[2][c.i] = z2;
-        double chi, cint, K;
-        if (!mixture(P, z0, z1, z2, chi, cint, K)) vmix = 1;
-        B.K[c.i] = K;
-        B.chi[c.i] = chi;
-        B.icpt[c.i] = fma(chi, P.mu_ref, cint);
-        if (P.phase_only) {
-            B.c[cur ^ 1][c.i] = fma(chi, mu, cint);
-            B.mu[cur ^ 1][c.i] = mu;
         }
     }
     double v[3] = {vchange, vmix, vsimp};
@@ -296,14 +386,17 @@ __device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
     const DevBufs& B = a.B;
     double* const* tp = B.phi[cur ^ 1];
     double vmix = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        double chi, cint, K;
-        if (!mixture(P, tp[0][c.i], tp[1][c.i], tp[2][c.i], chi, cint, K)) vmix = 1;
-        B.K[c.i] = K;
-        B.chi[c.i] = chi;
-        B.icpt[c.i] = fma(chi, P.mu_ref, cint);
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            double chi, cint, K;
+            if (!mixture(P, tp[0][i], tp[1][i], tp[2][i], chi, cint, K)) vmix = 1;
+            B.K[i] = K;
+            B.chi[i] = chi;
+            B.icpt[i] = fma(chi, P.mu_ref, cint);
+        }
     }
     double v[1] = {vmix};
     if (!red.reduce<1>(v, kMax, kTagMix)) return false;
@@ -316,28 +409,51 @@ __device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
 __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double& rhs2, double& rz, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    const double* mu = B.mu[cur];
-    const double* cold = B.c[cur];
     double s0 = 0, s1 = 0, s2 = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const Faces f = faces_at(P, B.K, c);
-        const double chi = B.chi[c.i];
-        const double u = mu[c.i] - P.mu_ref;
-        const double Au = apply_at(chi, dt, f, u, mu[c.iw] - P.mu_ref, mu[c.ie] - P.mu_ref, mu[c.is] - P.mu_ref,
-                                   mu[c.in] - P.mu_ref);
-        const double diag = chi + dt * (f.w0 + f.w1 + f.w2 + f.w3);
-        const double rhs = cold[c.i] - B.icpt[c.i];
-        const double r = rhs - Au;
-        const double z = r / diag;
-        B.x[c.i] = u;
-        B.r[c.i] = r;
-        B.z[c.i] = z;
-        B.diag[c.i] = diag;
-        s0 += rhs * rhs;
-        s1 += r * z;
-        s2 += r * r;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+        const S2 K = load_s2(B.K, c);
+        S2 u = load_s2(B.mu[cur], c);
+        const double chi0 = B.chi[c.i0], ic0 = B.icpt[c.i0], cold0 = B.c[cur][c.i0];
+        double chi1 = 0, ic1 = 0, cold1 = 0;
+        if (c.v1) {
+            chi1 = B.chi[c.i1];
+            ic1 = B.icpt[c.i1];
+            cold1 = B.c[cur][c.i1];
+        }
+        u.c0 -= P.mu_ref; u.c1 -= P.mu_ref; u.w0 -= P.mu_ref; u.e0 -= P.mu_ref;
+        u.w1 -= P.mu_ref; u.e1 -= P.mu_ref; u.s0 -= P.mu_ref; u.n1 -= P.mu_ref;
+        {
+            const Faces f = faces0(P, K, c);
+            const double Au = apply0(chi0, dt, f, u);
+            const double diag = chi0 + dt * (f.w0 + f.w1 + f.w2 + f.w3);
+            const double rhs = cold0 - ic0;
+            const double r = rhs - Au;
+            const double z = r / diag;
+            B.x[c.i0] = u.c0;
+            B.r[c.i0] = r;
+            B.z[c.i0] = z;
+            B.diag[c.i0] = diag;
+            s0 += rhs * rhs;
+            s1 += r * z;
+            s2 += r * r;
+        }
+        if (c.v1) {
+            const Faces f = faces1(P, K, c);
+            const double Au = apply1(chi1, dt, f, u);
+            const double diag = chi1 + dt * (f.w0 + f.w1 + f.w2 + f.w3);
+            const double rhs = cold1 - ic1;
+            const double r = rhs - Au;
+            const double z = r / diag;
+            B.x[c.i1] = u.c1;
+            B.r[c.i1] = r;
+            B.z[c.i1] = z;
+            B.diag[c.i1] = diag;
+            s0 += rhs * rhs;
+            s1 += r * z;
+            s2 += r * r;
+        }
     }
     double v[3] = {s0, s1, s2};
     if (!red.reduce<3>(v, OPS3(kSum, kSum, kSum), kTagSetup)) return false;
@@ -351,32 +467,36 @@ __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double
 __device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    const double* z = B.z;
-    const double* po = B.p[pout ^ 1];
     double* pn = B.p[pout];
     double s = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const Faces f = faces_at(P, B.K, c);
-        double pc, pw, pe, ps, pnn;
-        if (first) {
-            pc = z[c.i];
-            pw = z[c.iw];
-            pe = z[c.ie];
-            ps = z[c.is];
-            pnn = z[c.in];
-        } else {
-            pc = z[c.i] + beta * po[c.i];
-            pw = z[c.iw] + beta * po[c.iw];
-            pe = z[c.ie] + beta * po[c.ie];
-            ps = z[c.is] + beta * po[c.is];
-            pnn = z[c.in] + beta * po[c.in];
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+        const S2 K = load_s2(B.K, c);
+        S2 p = load_s2(B.z, c);
+        if (!first) {
+            const S2 po = load_s2(B.p[pout ^ 1], c);
+            p.c0 = p.c0 + beta * po.c0;
+            p.c1 = p.c1 + beta * po.c1;
+            p.w0 = p.w0 + beta * po.w0;
+            p.e0 = p.e0 + beta * po.e0;
+            p.w1 = p.w1 + beta * po.w1;
+            p.e1 = p.e1 + beta * po.e1;
+            p.s0 = p.s0 + beta * po.s0;
+            p.n1 = p.n1 + beta * po.n1;
         }
-        const double Ap = apply_at(B.chi[c.i], dt, f, pc, pw, pe, ps, pnn);
-        pn[c.i] = pc;
-        B.Ap[c.i] = Ap;
-        s += pc * Ap;
+        const double chi0 = B.chi[c.i0];
+        const double chi1 = c.v1 ? B.chi[c.i1] : 0.0;
+        const double Ap0 = apply0(chi0, dt, faces0(P, K, c), p);
+        pn[c.i0] = p.c0;
+        B.Ap[c.i0] = Ap0;
+        s += p.c0 * Ap0;
+        if (c.v1) {
+            const double Ap1 = apply1(chi1, dt, faces1(P, K, c), p);
+            pn[c.i1] = p.c1;
+            B.Ap[c.i1] = Ap1;
+            s += p.c1 * Ap1;
+        }
     }
     double v[1] = {s};
     if (!red.reduce<1>(v, kSum, kTagApply)) return false;
@@ -390,17 +510,34 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
     const DevBufs& B = a.B;
     const double* p = B.p[pcur];
     double s0 = 0, s1 = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const double x = B.x[c.i] + alpha * p[c.i];
-        const double r = B.r[c.i] - alpha * B.Ap[c.i];
-        const double z = r / B.diag[c.i];
-        B.x[c.i] = x;
-        B.r[c.i] = r;
-        B.z[c.i] = z;
-        s0 += r * z;
-        s1 += r * r;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+        const double x0 = B.x[c.i0], p0 = p[c.i0], r0 = B.r[c.i0], A0 = B.Ap[c.i0], d0 = B.diag[c.i0];
+        double x1 = 0, p1 = 0, r1 = 0, A1 = 0, d1 = 1;
+        if (c.v1) {
+            x1 = B.x[c.i1];
+            p1 = p[c.i1];
+            r1 = B.r[c.i1];
+            A1 = B.Ap[c.i1];
+            d1 = B.diag[c.i1];
+        }
+        {
+            const double x = x0 + alpha * p0, r = r0 - alpha * A0, z = r / d0;
+            B.x[c.i0] = x;
+            B.r[c.i0] = r;
+            B.z[c.i0] = z;
+            s0 += r * z;
+            s1 += r * r;
+        }
+        if (c.v1) {
+            const double x = x1 + alpha * p1, r = r1 - alpha * A1, z = r / d1;
+            B.x[c.i1] = x;
+            B.r[c.i1] = r;
+            B.z[c.i1] = z;
+            s0 += r * z;
+            s1 += r * r;
+        }
     }
     double v[2] = {s0, s1};
     if (!red.reduce<2>(v, OPS2(kSum, kSum), kTagUpdate)) return false;
@@ -413,16 +550,29 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
 __device__ bool phase_true_residual(const KArgs& a, Red& red, int cur, double dt, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    const double* x = B.x;
     double s = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const Faces f = faces_at(P, B.K, c);
-        const double Ax = apply_at(B.chi[c.i], dt, f, x[c.i], x[c.iw], x[c.ie], x[c.is], x[c.in]);
-        const double r = (B.c[cur][c.i] - B.icpt[c.i]) - Ax;
-        B.r[c.i] = r;
-        s += r * r;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+        const S2 K = load_s2(B.K, c);
+        const S2 x = load_s2(B.x, c);
+        const double chi0 = B.chi[c.i0], ic0 = B.icpt[c.i0], c0 = B.c[cur][c.i0];
+        double chi1 = 0, ic1 = 0, c1 = 0;
+        if (c.v1) {
+            chi1 = B.chi[c.i1];
+            ic1 = B.icpt[c.i1];
+            c1 = B.c[cur][c.i1];
+        }
+        {
+            const double r = (c0 - ic0) - apply0(chi0, dt, faces0(P, K, c), x);
+            B.r[c.i0] = r;
+            s += r * r;
+        }
+        if (c.v1) {
+            const double r = (c1 - ic1) - apply1(chi1, dt, faces1(P, K, c), x);
+            B.r[c.i1] = r;
+            s += r * r;
+        }
     }
     double v[1] = {s};
     if (!red.reduce<1>(v, kSum, kTagTrueRes)) return false;
@@ -435,13 +585,16 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double s = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const double r = B.r[c.i];
-        const double z = r / B.diag[c.i];
-        B.z[c.i] = z;
-        s += r * z;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            const double r = B.r[i];
+            const double z = r / B.diag[i];
+            B.z[i] = z;
+            s += r * z;
+        }
     }
     double v[1] = {s};
     if (!red.reduce<1>(v, kSum, kTagReset)) return false;
@@ -450,33 +603,51 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
 }
 
 // FINAL: carbon update, closure and mu (pearl_serial.cpp:1082-1093) fused with
-// valid_state, total_carbon and reduced_energy of the trial state.
-// Reduction: {closure max, bad max, carbon sum, energy sum}.
+// valid_state, total_carbon and reduced_energy of the trial state.  The two
+// cells of a thread are processed one after the other (this phase carries the
+// most live values).  Reduction: {closure max, bad max, carbon sum, energy sum}.
 __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double& closure, bool& bad,
                             double& mass, double& energy) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const int tr = cur ^ 1;
-    const double* x = B.x;
     const double* const* tp = B.phi[tr];
+    const double* x = B.x;
+    const double* K = B.K;
     double vclos = 0, vbad = 0, vmass = 0, ven = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const Faces f = faces_at(P, B.K, c);
-        const double u = x[c.i];
-        const double change =
-            dt * (f.w0 * (x[c.iw] - u) + f.w1 * (x[c.ie] - u) + f.w2 * (x[c.is] - u) + f.w3 * (x[c.in] - u));
-        const double chi = B.chi[c.i], icpt = B.icpt[c.i];
-        const double cn = B.c[cur][c.i] + change;
-        vclos = fmax(vclos, fabs(cn - (icpt + chi * u)));
-        const double mun = P.mu_ref + (cn - icpt) / chi;
-        B.c[tr][c.i] = cn;
-        B.mu[tr][c.i] = mun;
-        const double q0 = tp[0][c.i], q1 = tp[1][c.i], q2 = tp[2][c.i];
-        if (bad_cell(P, q0, q1, q2, cn, mun)) vbad = 1;
-        vmass += cn;
-        ven += energy_cell(P, c, q0, q1, q2, tp, cn, chi, icpt);
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !c.v1) break;
+            const int y = c.y0 + k;
+            const size_t i = k ? c.i1 : c.i0;
+            const size_t iw = k ? c.iw1 : c.iw0, ie = k ? c.ie1 : c.ie0;
+            const size_t is = k ? c.i0 : c.is0;
+            const size_t in = k ? c.in1 : (c.v1 ? c.i1 : c.i0);
+            const bool has_n = y < P.ny - 1;
+            Faces f;
+            const double kc = K[i];
+            f.w0 = face_x(P, kc, K[iw]);
+            f.w1 = face_x(P, kc, K[ie]);
+            f.w2 = face_y(P, kc, K[is]);
+            f.w3 = face_y(P, kc, K[in]);
+            if (y == 0) f.w2 = 0;
+            if (!has_n) f.w3 = 0;
+            const double u = x[i];
+            const double cn = B.c[cur][i] + flux_at(dt, f, u, x[iw], x[ie], x[is], x[in]);
+            const double chi = B.chi[i], icpt = B.icpt[i];
+            vclos = fmax(vclos, fabs(cn - (icpt + chi * u)));
+            const double mun = P.mu_ref + (cn - icpt) / chi;
+            B.c[tr][i] = cn;
+            B.mu[tr][i] = mun;
+            const Phi3 q = load_phi(tp, i), e = load_phi(tp, ie);
+            const Phi3 n = has_n ? load_phi(tp, in) : Phi3{0, 0, 0};
+            if (bad_cell(P, q, cn, mun)) vbad = 1;
+            vmass += cn;
+            ven += energy_cell(P, q, e, n, has_n, cn, chi, icpt);
+        }
     }
     double v[4] = {vclos, vbad, vmass, ven};
     if (!red.reduce<4>(v, OPS4(kMax, kMax, kSum, kSum), kTagFinal)) return false;
@@ -487,25 +658,52 @@ __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double
     return true;
 }
 
+// Energy and validity of state set `s` whose mixture is recomputed from phi
+// (ENERGY) or taken from the trial mixture buffers (phase-only FINAL).
+// Accumulates in the same order as phase_final, so equal states give equal sums.
+template <bool kFromBuffers>
+__device__ void energy_sweep(const KArgs& a, int s, double& ven, double& vmass, double& vmix, double& vbad) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[s];
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !c.v1) break;
+            const size_t i = k ? c.i1 : c.i0;
+            const size_t ie = k ? c.ie1 : c.ie0;
+            const int y = c.y0 + k;
+            const bool has_n = y < P.ny - 1;
+            const size_t in = k ? c.in1 : c.i1;
+            const Phi3 q = load_phi(ph, i), e = load_phi(ph, ie);
+            const Phi3 n = has_n ? load_phi(ph, in) : Phi3{0, 0, 0};
+            double chi = 1, icpt = 0;
+            if (kFromBuffers) {
+                chi = B.chi[i];
+                icpt = B.icpt[i];
+            } else if (!P.phase_only) {
+                double cint, K;
+                if (!mixture(P, q.a, q.t, q.g, chi, cint, K)) vmix = 1;
+                icpt = fma(chi, P.mu_ref, cint);
+            }
+            const double cc = B.c[s][i];
+            ven += energy_cell(P, q, e, n, has_n, cc, chi, icpt);
+            vmass += cc;
+            if (bad_cell(P, q, cc, B.mu[s][i])) vbad = 1;
+        }
+    }
+}
+
 // PHASE_ONLY FINAL: valid_state and reduced_energy of the trial state whose
 // carbon and mu were written by PROPOSE.  Reduction: {bad max, energy sum}.
 __device__ bool phase_final_phase_only(const KArgs& a, Red& red, int cur, bool& bad, double& energy) {
-    const DevParams& P = a.P;
-    const DevBufs& B = a.B;
-    const int tr = cur ^ 1;
-    const double* const* tp = B.phi[tr];
-    double vbad = 0, ven = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const double q0 = tp[0][c.i], q1 = tp[1][c.i], q2 = tp[2][c.i];
-        if (bad_cell(P, q0, q1, q2, B.c[tr][c.i], B.mu[tr][c.i])) vbad = 1;
-        ven += energy_cell(P, c, q0, q1, q2, tp, 0.0, B.chi[c.i], B.icpt[c.i]);
-    }
+    double ven = 0, vmass = 0, vmix = 0, vbad = 0;
+    energy_sweep<true>(a, cur ^ 1, ven, vmass, vmix, vbad);
     double v[2] = {vbad, ven};
     if (!red.reduce<2>(v, OPS2(kMax, kSum), kTagFinalPhaseOnly)) return false;
     bad = v[0] != 0;
-    energy = v[1] * P.dx * P.dy;
+    energy = v[1] * a.P.dx * a.P.dy;
     return true;
 }
 
@@ -514,27 +712,12 @@ __device__ bool phase_final_phase_only(const KArgs& a, Red& red, int cur, bool& 
 // valid_state.  Reduction: {energy sum, carbon sum, mixture invalid, bad}.
 __device__ bool phase_energy(const KArgs& a, Red& red, int s, double& energy, double& mass, bool& mixbad,
                              bool& bad) {
-    const DevParams& P = a.P;
-    const DevBufs& B = a.B;
-    const double* const* ph = B.phi[s];
     double ven = 0, vmass = 0, vmix = 0, vbad = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const double q0 = ph[0][c.i], q1 = ph[1][c.i], q2 = ph[2][c.i];
-        double chi = 1, cint = 0, K;
-        if (!P.phase_only) {
-            if (!mixture(P, q0, q1, q2, chi, cint, K)) vmix = 1;
-        }
-        const double cc = B.c[s][c.i];
-        ven += energy_cell(P, c, q0, q1, q2, ph, cc, chi, fma(chi, P.mu_ref, cint));
-        vmass += cc;
-        if (bad_cell(P, q0, q1, q2, cc, B.mu[s][c.i])) vbad = 1;
-    }
+    energy_sweep<false>(a, s, ven, vmass, vmix, vbad);
     double v[4] = {ven, vmass, vmix, vbad};
     if (!red.reduce<4>(v, OPS4(kSum, kSum, kMax, kMax), kTagEnergy)) return false;
-    energy = v[0] * P.dx * P.dy;
-    mass = v[1] * P.dx * P.dy;
+    energy = v[0] * a.P.dx * a.P.dy;
+    mass = v[1] * a.P.dx * a.P.dy;
     mixbad = v[2] != 0;
     bad = v[3] != 0;
     return true;
@@ -547,8 +730,7 @@ __device__ __forceinline__ void set_error(Ctl* ctl, int status, int why) {
 }
 
 // Implicit diffusion: SETUP, Jacobi-PCG (pearl_serial.cpp:1047-1080) and FINAL.
-// Returns false only on a device-wait timeout.  Sets ok/it/residual and, when
-// the solve converged, the FINAL reductions.
+// Returns false only on a device-wait timeout.
 struct DiffusionOut {
     bool ok;
     int it;
@@ -717,11 +899,15 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     const int cur = st.cur;
     const double* g = B.phi[cur][2];
     double local = -1;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok || c.y == P.ny - 1) continue;
-        const double av = 1 - 2 * g[c.i], bv = 1 - 2 * g[c.in];
-        if (av >= 0 && bv < 0) local = fmax(local, ((c.y + 1) - .5 + av / (av - bv)) * P.dy);
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            const int y = c.y0 + k;
+            if (!(k ? c.v1 : c.v0) || y == P.ny - 1) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            const double av = 1 - 2 * g[i], bv = 1 - 2 * g[i + P.pitch];
+            if (av >= 0 && bv < 0) local = fmax(local, ((y + 1) - .5 + av / (av - bv)) * P.dy);
+        }
     }
     double v1[1] = {local};
     if (!red.reduce<1>(v1, kMax, kTagShift)) return false;
@@ -730,10 +916,12 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     if (front < a.shift_trigger) return true;
     const int rows = (int)floor((front - a.shift_target) / P.dy);
     double gmax = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok || c.y >= rows) continue;
-        gmax = fmax(gmax, g[c.i]);
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0) || c.y0 + k >= rows) continue;
+            gmax = fmax(gmax, g[k ? c.i1 : c.i0]);
+        }
     }
     double v2[1] = {gmax};
     if (!red.reduce<1>(v2, kMax, kTagShift)) return false;
@@ -747,31 +935,35 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     }
     const int nw = cur ^ 1;
     double removed = 0, vmix = 0, vnonfin = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        if (c.y < rows) removed += B.c[cur][c.i] * P.dx * P.dy;
-        double q0, q1, q2, cc;
-        if (c.y + rows < P.ny) {
-            const size_t j = c.i + (size_t)rows * P.pitch;
-            q0 = B.phi[cur][0][j];
-            q1 = B.phi[cur][1][j];
-            q2 = B.phi[cur][2][j];
-            cc = B.c[cur][j];
-        } else {
-            q0 = 0;
-            q1 = 0;
-            q2 = 1;
-            cc = a.shift_c_gamma;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const int y = c.y0 + k;
+            const size_t i = k ? c.i1 : c.i0;
+            if (y < rows) removed += B.c[cur][i] * P.dx * P.dy;
+            double q0, q1, q2, cc;
+            if (y + rows < P.ny) {
+                const size_t j = i + (size_t)rows * P.pitch;
+                q0 = B.phi[cur][0][j];
+                q1 = B.phi[cur][1][j];
+                q2 = B.phi[cur][2][j];
+                cc = B.c[cur][j];
+            } else {
+                q0 = 0;
+                q1 = 0;
+                q2 = 1;
+                cc = a.shift_c_gamma;
+            }
+            B.phi[nw][0][i] = q0;
+            B.phi[nw][1][i] = q1;
+            B.phi[nw][2][i] = q2;
+            B.c[nw][i] = cc;
+            double chi, cint, K;
+            if (!mixture(P, q0, q1, q2, chi, cint, K)) vmix = 1;
+            if (!isfinite(cc)) vnonfin = 1;
+            B.mu[nw][i] = (cc - cint) / chi;  // close_mu / reconstruct_mu (:139-142, :789-792)
         }
-        B.phi[nw][0][c.i] = q0;
-        B.phi[nw][1][c.i] = q1;
-        B.phi[nw][2][c.i] = q2;
-        B.c[nw][c.i] = cc;
-        double chi, cint, K;
-        if (!mixture(P, q0, q1, q2, chi, cint, K)) vmix = 1;
-        if (!isfinite(cc)) vnonfin = 1;
-        B.mu[nw][c.i] = (cc - cint) / chi;  // close_mu / reconstruct_mu (:139-142, :789-792)
     }
     double v3[3] = {removed, vmix, vnonfin};
     if (!red.reduce<3>(v3, OPS3(kSum, kMax, kMax), kTagShift)) return false;
@@ -800,15 +992,18 @@ __device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
     const DevBufs& B = a.B;
     const double* const* ph = B.phi[s];
     double minc = 1e300, maxc = -1e300, minmu = 1e300, maxmu = -1e300, sumerr = 0;
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x) {
-        const Cell c = cell_of(P, t);
-        if (!c.ok) continue;
-        const double cc = B.c[s][c.i], mu = B.mu[s][c.i];
-        minc = fmin(minc, cc);
-        maxc = fmax(maxc, cc);
-        minmu = fmin(minmu, mu);
-        maxmu = fmax(maxmu, mu);
-        sumerr = fmax(sumerr, fabs(ph[0][c.i] + ph[1][c.i] + ph[2][c.i] - 1));
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            const double cc = B.c[s][i], mu = B.mu[s][i];
+            minc = fmin(minc, cc);
+            maxc = fmax(maxc, cc);
+            minmu = fmin(minmu, mu);
+            maxmu = fmax(maxmu, mu);
+            sumerr = fmax(sumerr, fabs(ph[0][i] + ph[1][i] + ph[2][i] - 1));
+        }
     }
     double v[5] = {minc, maxc, minmu, maxmu, sumerr};
     if (!red.reduce<5>(v, OPS5(kMin, kMax, kMin, kMax, kMax), kTagSnapshot)) return false;
@@ -938,6 +1133,21 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
     }
 }
 
+// Self-test of the exact constant-divisor division: counts elements where
+// div_by(a, b, RN(1/b)) differs bitwise from the IEEE quotient a/b.
+__global__ void division_selftest_kernel(const double* a, const double* b, const double* rb, long long n,
+                                         unsigned long long* mismatches, int use_exact) {
+    DevParams P;
+    P.exact_div = use_exact;
+    unsigned long long bad = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double q = div_by(P, a[i], b[i], rb[i]);
+        const double ref = a[i] / b[i];
+        if (__double_as_longlong(q) != __double_as_longlong(ref)) ++bad;
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+
 }  // namespace pearl_gpu
 
 // ====================================================================== host side
@@ -1020,7 +1230,7 @@ void fill_dev_params(pearl_gpu_ctx* ctx) {
     P.ny = ctx->ny;
     P.pitch = ctx->pitch;
     P.ntx = (ctx->nx + kTileX - 1) / kTileX;
-    P.nty = (ctx->ny + kTileY - 1) / kTileY;
+    P.nty = (ctx->ny + kTileRows - 1) / kTileRows;
     P.ntiles = P.ntx * P.nty;
     P.dx = p->dx;
     P.dy = p->dy;
@@ -1065,6 +1275,19 @@ void fill_dev_params(pearl_gpu_ctx* ctx) {
     P.max_retries = p->max_retries;
     P.check_energy = p->check_energy;
     P.phase_only = p->phase_only;
+    // reciprocals of the constant divisors (RN(1/b), host IEEE division)
+    P.r_Vm = 1.0 / P.Vm;
+    P.r_dx = 1.0 / P.dx;
+    P.r_dy = 1.0 / P.dy;
+    P.r_dx2 = 1.0 / P.dx2;
+    P.r_dy2 = 1.0 / P.dy2;
+    P.r_3 = 1.0 / 3.0;
+    for (int i = 0; i < 3; ++i) P.r_two_A[i] = 1.0 / P.two_A[i];
+    const double divisors[] = {P.Vm, P.dx, P.dy, P.dx2, P.dy2, 3.0, P.two_A[0], P.two_A[1], P.two_A[2]};
+    const double recips[] = {P.r_Vm, P.r_dx, P.r_dy, P.r_dx2, P.r_dy2, P.r_3, P.r_two_A[0], P.r_two_A[1], P.r_two_A[2]};
+    P.exact_div = 1;
+    for (int i = 0; i < 9; ++i)
+        if (std::fpclassify(divisors[i]) != FP_NORMAL || std::fpclassify(recips[i]) != FP_NORMAL) P.exact_div = 0;
 }
 
 int pull_ctl(pearl_gpu_ctx* ctx) {
@@ -1468,6 +1691,37 @@ int pearl_gpu_valid_state(pearl_gpu_ctx* ctx, int* valid) {
     if (rc) return rc;
     *valid = ctx->h_ctl->iout[1] ? 0 : 1;
     return PEARL_OK;
+}
+
+int pearl_gpu_selftest_division(int device, const double* a, const double* b, long long n,
+                                unsigned long long* mismatches) {
+    if (!a || !b || n < 0 || !mismatches) return PEARL_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return PEARL_ERR_NO_DEVICE;
+    std::vector<double> rb((size_t)n);
+    for (long long i = 0; i < n; ++i) rb[(size_t)i] = 1.0 / b[i];
+    double *da = nullptr, *db = nullptr, *drb = nullptr;
+    unsigned long long* dm = nullptr;
+    const size_t bytes = (size_t)n * sizeof(double);
+    int rc = PEARL_OK;
+    if (cudaMalloc(&da, bytes) != cudaSuccess || cudaMalloc(&db, bytes) != cudaSuccess ||
+        cudaMalloc(&drb, bytes) != cudaSuccess || cudaMalloc(&dm, sizeof(unsigned long long)) != cudaSuccess)
+        rc = PEARL_ERR_CUDA;
+    if (rc == PEARL_OK && (cudaMemcpy(da, a, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+                           cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+                           cudaMemcpy(drb, rb.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+                           cudaMemset(dm, 0, sizeof(unsigned long long)) != cudaSuccess))
+        rc = PEARL_ERR_CUDA;
+    if (rc == PEARL_OK) {
+        division_selftest_kernel<<<1184, 256>>>(da, db, drb, n, dm, 1);
+        if (cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(mismatches, dm, sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = PEARL_ERR_CUDA;
+    }
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(drb);
+    cudaFree(dm);
+    return rc;
 }
 
 int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts) {

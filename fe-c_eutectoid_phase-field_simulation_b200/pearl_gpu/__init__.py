@@ -107,6 +107,7 @@ EXPORTS = [
     "pearl_gpu_maybe_shift", "pearl_gpu_snapshot", "pearl_gpu_propose_phi", "pearl_gpu_upload_trial_phi",
     "pearl_gpu_implicit_diffusion", "pearl_gpu_download_trial", "pearl_gpu_energy_mass", "pearl_gpu_valid_state",
     "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats", "pearl_gpu_phase_times",
+    "pearl_gpu_selftest_division",
 ]
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
@@ -150,9 +151,21 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_last_error.restype = C.c_char_p
     L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
     L.pearl_gpu_phase_times.argtypes = [V, DP, C.POINTER(C.c_longlong)]
+    L.pearl_gpu_selftest_division.argtypes = [C.c_int, DP, DP, C.c_longlong, C.POINTER(C.c_ulonglong)]
     if path is None:
         _lib = L
     return L
+
+
+def selftest_division(a: np.ndarray, b: np.ndarray, device: int = 0) -> int:
+    """Number of elements where the device's exact constant-divisor division differs from a/b."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = C.c_ulonglong(0)
+    rc = library().pearl_gpu_selftest_division(device, _p(a), _p(b), a.size, C.byref(n))
+    if rc:
+        raise PearlError(rc, STATUS.get(rc, str(rc)))
+    return int(n.value)
 
 
 class PearlError(RuntimeError):

@@ -182,6 +182,13 @@ int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* kernel_launches, int* g
  * 11 snapshot.  Each slot covers its sweep, reduction and grid barrier. */
 int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts);
 
+/* Self-test of the device's exact division by a precomputed reciprocal, which
+ * the kernels use for every constant divisor of the reference's formulas
+ * (Vm, dx, dy, dx*dx, dy*dy, 3, 2A): counts the n elements where it differs
+ * bitwise from IEEE a[i]/b[i] on `device`.  No reference counterpart. */
+int pearl_gpu_selftest_division(int device, const double* a, const double* b, long long n,
+                                unsigned long long* mismatches);
+
 #ifdef __cplusplus
 }
 #endif
