@@ -26,6 +26,7 @@ STATUS = {
     7: "Simplex projection failed", 8: "configured max_steps reached before end_time",
     9: "device wait limit exceeded", 10: "unsafe shift: removed strip contains gamma",
     11: "Nonfinite total carbon", 12: "no CUDA device",
+    13: "domain exceeds the no-allocation scratch limit of 262144 cells",
 }
 
 
@@ -107,7 +108,7 @@ EXPORTS = [
     "pearl_gpu_maybe_shift", "pearl_gpu_snapshot", "pearl_gpu_propose_phi", "pearl_gpu_upload_trial_phi",
     "pearl_gpu_implicit_diffusion", "pearl_gpu_download_trial", "pearl_gpu_energy_mass", "pearl_gpu_valid_state",
     "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats", "pearl_gpu_phase_times",
-    "pearl_gpu_selftest_division",
+    "pearl_gpu_selftest_division", "pearl_gpu_advance_noalloc",
 ]
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
@@ -152,6 +153,8 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
     L.pearl_gpu_phase_times.argtypes = [V, DP, C.POINTER(C.c_longlong)]
     L.pearl_gpu_selftest_division.argtypes = [C.c_int, DP, DP, C.c_longlong, C.POINTER(C.c_ulonglong)]
+    L.pearl_gpu_advance_noalloc.argtypes = [C.POINTER(PearlParams), C.c_int, C.c_int, V, V, V,
+                                            C.POINTER(PearlScalars), D, C.POINTER(PearlStepInfo), V]
     if path is None:
         _lib = L
     return L

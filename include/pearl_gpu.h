@@ -102,7 +102,8 @@ typedef enum pearl_status {
     PEARL_ERR_DEVICE_WAIT = 9,            /* a bounded device-side wait ran out (no reference counterpart) */
     PEARL_ERR_UNSAFE_SHIFT = 10,          /* "unsafe shift: removed strip contains gamma" (:2068) */
     PEARL_ERR_NONFINITE_CARBON = 11,      /* "Nonfinite total carbon" (:140) */
-    PEARL_ERR_NO_DEVICE = 12
+    PEARL_ERR_NO_DEVICE = 12,
+    PEARL_ERR_TOO_LARGE = 13              /* domain exceeds the no-allocation scratch (no reference counterpart) */
 } pearl_status;
 
 /* Rejection reason <why> of the last attempt (pearl_serial.cpp:1133-1160). */
@@ -188,6 +189,30 @@ int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* count
  * bitwise from IEEE a[i]/b[i] on `device`.  No reference counterpart. */
 int pearl_gpu_selftest_division(int device, const double* a, const double* b, long long n,
                                 unsigned long long* mismatches);
+
+/* One accepted step (as pearl_gpu_advance) for callers that cannot allocate
+ * device memory: code whose GPU memory is owned by another allocator (a
+ * framework's caching pool or a fixed memory budget) and latency-critical
+ * loops that must avoid cudaMalloc/cudaFree, which can synchronise the device.
+ * No counterpart in the reference.
+ *
+ * The caller owns the state in device memory as dense planes of nx*ny doubles
+ * (row-major, x fastest): d_phi holds the alpha, theta and gamma planes back
+ * to back, d_carbon and d_mu one plane each.  They are read as the current
+ * state and overwritten with the accepted one; *scalars is read and updated.
+ * Runs on the calling thread's current device and on `stream` (NULL = legacy
+ * default stream) and returns after the step has finished.
+ *
+ * All scratch comes from one array compiled into the library (about 32 MB,
+ * held by every GPU that loads the library until the process exits), so
+ * nx*ny is limited to 262144 cells; larger domains return PEARL_ERR_TOO_LARGE.
+ * The first call on each device looks up that array's device address; make
+ * that first call before any stream capture.  All calls on a device share the
+ * same scratch, so calls that overlap on the GPU (other streams or threads)
+ * race and must be serialised by the caller. */
+int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double* d_phi, double* d_carbon,
+                              double* d_mu, pearl_scalars* scalars, double stop_time, pearl_step_info* out,
+                              void* stream);
 
 #ifdef __cplusplus
 }
