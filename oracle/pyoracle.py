@@ -137,6 +137,11 @@ class Port(_Lib):
         L.po_interface_energy_only.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP]
         L.po_interface_energy_only.restype = D
         L.po_close_mu.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP]
+        L.po_psi.argtypes = [C.POINTER(PoParams), C.c_int, D]
+        L.po_psi.restype = D
+
+    def psi(self, params, phase: int, mu: float) -> float:
+        return self.lib.po_psi(C.byref(_params(params)), phase, mu)
 
     def propose_phi(self, params, phi, mu, dt):
         ny, nx = mu.shape
