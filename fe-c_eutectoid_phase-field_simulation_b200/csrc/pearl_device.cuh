@@ -99,7 +99,7 @@ struct Ctl {
     pearl_step_info last;
     long long steps, cg_total;
     int cg_peak, reached_stop;
-    double out[8];
+    double out[16];
     int iout[4];
     // per-phase device time of the last launch, measured by block 0 between
     // consecutive grid barriers (phase compute + reduction + barrier wait)
@@ -109,7 +109,7 @@ struct Ctl {
 
 enum PhaseTag : int {
     kTagPropose = 0, kTagSetup, kTagApply, kTagUpdate, kTagTrueRes, kTagReset, kTagFinal, kTagEnergy,
-    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagCount
+    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagSmooth, kTagInit, kTagCount
 };
 
 // ---------------------------------------------------------------- thermodynamics

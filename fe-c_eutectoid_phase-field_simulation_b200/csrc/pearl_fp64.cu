@@ -42,6 +42,9 @@ enum Mode : int {
     kModeValid = 5,
     kModeSnapshot = 6,
     kModeMaybeShift = 7,
+    kModeSmooth = 8,
+    kModeMixSums = 9,
+    kModeInitComposition = 10,
 };
 
 struct KArgs {
@@ -51,6 +54,9 @@ struct KArgs {
     double dt;  // diagnostic modes
     pearl_run_limits L;
     double shift_trigger, shift_target, shift_c_gamma;
+    int smooth_max_steps, smooth_min_steps;
+    double smooth_energy_rtol, smooth_max_phase_change;
+    double init_mu;
 };
 
 // The two cells (x, y0) and (x, y0+1) of one thread in tile t.
@@ -986,6 +992,281 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     return true;
 }
 
+// ------------------------------------------------------------------ initialisation
+// Interface-only energy density of one cell (interface_energy_only,
+// pearl_serial.cpp:822-842), without the final dx*dy.
+__device__ __forceinline__ double interface_energy_cell(const DevParams& P, const Phi3& q, const Phi3& e,
+                                                        const Phi3& n, bool has_n) {
+    double t = P.obs * (q.a * q.t + q.a * q.g + q.t * q.g) + P.tr * q.a * q.t * q.g;
+    double z = div_by(P, q.a * e.t - e.a * q.t, P.dx, P.r_dx);
+    t += P.eps_sigma * z * z;
+    z = div_by(P, q.a * e.g - e.a * q.g, P.dx, P.r_dx);
+    t += P.eps_sigma * z * z;
+    z = div_by(P, q.t * e.g - e.t * q.g, P.dx, P.r_dx);
+    t += P.eps_sigma * z * z;
+    if (has_n) {
+        z = div_by(P, q.a * n.t - n.a * q.t, P.dy, P.r_dy);
+        t += P.eps_sigma * z * z;
+        z = div_by(P, q.a * n.g - n.a * q.g, P.dy, P.r_dy);
+        t += P.eps_sigma * z * z;
+        z = div_by(P, q.t * n.g - n.t * q.g, P.dy, P.r_dy);
+        t += P.eps_sigma * z * z;
+    }
+    return t;
+}
+
+// Interface-only energy of state set `s` plus its phase-fraction sums.
+// Reduction: {energy sum, sum phi_alpha, sum phi_theta, sum phi_gamma}.
+__device__ bool phase_interface_energy(const KArgs& a, Red& red, int s, double& energy, double* frac) {
+    const DevParams& P = a.P;
+    const double* const* ph = a.B.phi[s];
+    double ven = 0, f0 = 0, f1 = 0, f2 = 0;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !c.v1) break;
+            const size_t i = k ? c.i1 : c.i0;
+            const bool has_n = c.y0 + k < P.ny - 1;
+            const Phi3 q = load_phi(ph, i), e = load_phi(ph, k ? c.ie1 : c.ie0);
+            const Phi3 n = has_n ? load_phi(ph, k ? c.in1 : c.i1) : Phi3{0, 0, 0};
+            ven += interface_energy_cell(P, q, e, n, has_n);
+            f0 += q.a;
+            f1 += q.t;
+            f2 += q.g;
+        }
+    }
+    double v[4] = {ven, f0, f1, f2};
+    if (!red.reduce<4>(v, OPS4(kSum, kSum, kSum, kSum), kTagSmooth)) return false;
+    energy = v[0] * P.dx * P.dy;
+    const double cells = (double)P.nx * P.ny;
+    for (int k = 0; k < 3; ++k) frac[k] = v[1 + k] / cells;
+    return true;
+}
+
+// Capillary force of smooth_interface_only (pearl_serial.cpp:892-917) written
+// to the work planes x, r, z; reduction {max |force|}.
+__device__ bool phase_smooth_force(const KArgs& a, Red& red, int cur, double& force_max) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[cur];
+    double* fo[3] = {B.x, B.r, B.z};
+    double vmax = 0;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        if (!c.v0) continue;
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !c.v1) break;
+            const int y = c.y0 + k;
+            const size_t i = k ? c.i1 : c.i0;
+            const size_t iw = k ? c.iw1 : c.iw0, ie = k ? c.ie1 : c.ie0;
+            const size_t is = k ? c.i0 : c.is0, in = k ? c.in1 : c.i1;
+            const double q[3] = {ph[0][i], ph[1][i], ph[2][i]};
+            double f[3];
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa) {
+                const double qa1 = q[(aa + 1) % 3], qa2 = q[(aa + 2) % 3];
+                f[aa] = P.obs * (qa1 + qa2) + P.tr * qa1 * qa2;
+            }
+#pragma unroll
+            for (int dir = 0; dir < 4; ++dir) {
+                if ((dir == 2 && y == 0) || (dir == 3 && y == P.ny - 1)) continue;
+                const size_t j = dir == 0 ? iw : (dir == 1 ? ie : (dir == 2 ? is : in));
+                const double n[3] = {ph[0][j], ph[1][j], ph[2][j]};
+                const double d2 = dir < 2 ? P.dx2 : P.dy2, rd2 = dir < 2 ? P.r_dx2 : P.r_dy2;
+#pragma unroll
+                for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                    for (int b = aa + 1; b < 3; ++b) {
+                        const double w = div_by(P, P.two_eps_sigma * (q[aa] * n[b] - n[aa] * q[b]), d2, rd2);
+                        f[aa] += w * n[b];
+                        f[b] -= w * n[aa];
+                    }
+            }
+            const double mean = div_by(P, f[0] + f[1] + f[2], 3.0, P.r_3);
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa) {
+                const double v = f[aa] - mean;
+                fo[aa][i] = v;
+                vmax = fmax(vmax, fabs(v));
+            }
+        }
+    }
+    double v[1] = {vmax};
+    if (!red.reduce<1>(v, kMax, kTagSmooth)) return false;
+    force_max = v[0];
+    return true;
+}
+
+// Backtracking trial of smooth_interface_only (pearl_serial.cpp:925-933):
+// trial phi = project(phi - scale*force) into set cur^1.
+// Reduction: {max |dphi|, simplex failed}.
+__device__ bool phase_smooth_trial(const KArgs& a, Red& red, int cur, double scale, double& change, bool& bad) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[cur];
+    double* const* tp = B.phi[cur ^ 1];
+    double vch = 0, vbad = 0;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            const double q0 = ph[0][i], q1 = ph[1][i], q2 = ph[2][i];
+            double z0 = q0 - scale * B.x[i], z1 = q1 - scale * B.r[i], z2 = q2 - scale * B.z[i];
+            if (!(isfinite(z0) && isfinite(z1) && isfinite(z2)) || !project_simplex(P, z0, z1, z2)) vbad = 1;
+            vch = fmax(vch, fabs(z0 - q0));
+            vch = fmax(vch, fabs(z1 - q1));
+            vch = fmax(vch, fabs(z2 - q2));
+            tp[0][i] = z0;
+            tp[1][i] = z1;
+            tp[2][i] = z2;
+        }
+    }
+    double v[2] = {vch, vbad};
+    if (!red.reduce<2>(v, OPS2(kMax, kMax), kTagSmooth)) return false;
+    change = v[0];
+    bad = v[1] != 0;
+    return true;
+}
+
+// smooth_interface_only (pearl_serial.cpp:869-958) on the phase fields of the
+// current state.  Report layout in ctl->out: steps, converged, energy_initial,
+// energy_final, final_relative_energy_change, final_max_phase_change,
+// phase fractions before (3) and after (3).
+__device__ bool smooth(const KArgs& a, Red& red, StepState& st, double* rep) {
+    const DevParams& P = a.P;
+    Ctl* ctl = a.B.ctl;
+    const int max_steps = a.smooth_max_steps, min_steps = a.smooth_min_steps;
+    const double energy_rtol = a.smooth_energy_rtol, max_change = a.smooth_max_phase_change;
+    for (int k = 0; k < 12; ++k) rep[k] = 0;
+    double frac[3];
+    double e_init;
+    if (!phase_interface_energy(a, red, st.cur, e_init, frac)) return false;
+    for (int k = 0; k < 3; ++k) rep[6 + k] = frac[k];
+    rep[2] = e_init;
+    double previous = e_init;
+    const double base_scale = .12 * fmin(P.dx2, P.dy2) / P.eps_sigma;
+    int steps = 0;
+    bool converged = false;
+    double energy_final = 0, rel_final = 0, change_final = 0;
+    for (int step = 1; step <= max_steps; ++step) {
+        double force_max;
+        if (!phase_smooth_force(a, red, st.cur, force_max)) return false;
+        if (!isfinite(force_max)) {
+            set_error(ctl, PEARL_ERR_SMOOTHING, 1);
+            return false;
+        }
+        if (force_max == 0) {
+            steps = step - 1;
+            converged = true;
+            rel_final = 0;
+            change_final = 0;
+            break;
+        }
+        double scale = fmin(base_scale, max_change / force_max);
+        bool accepted = false;
+        double new_energy = previous, actual_change = 0;
+        for (int backtrack = 0; backtrack < 24 && !accepted; ++backtrack) {
+            bool bad;
+            if (!phase_smooth_trial(a, red, st.cur, scale, actual_change, bad)) return false;
+            if (bad) {
+                set_error(ctl, PEARL_ERR_SIMPLEX, 0);
+                return false;
+            }
+            double f3[3];
+            if (!phase_interface_energy(a, red, st.cur ^ 1, new_energy, f3)) return false;
+            double big = 1.0;
+            if (big < fabs(previous)) big = fabs(previous);
+            if (big < fabs(e_init)) big = fabs(e_init);
+            const double etol = 1e-14 * big;
+            if (isfinite(new_energy) && new_energy <= previous + etol)
+                accepted = true;
+            else
+                scale *= .5;
+        }
+        if (!accepted) {
+            set_error(ctl, PEARL_ERR_SMOOTHING, 2);
+            return false;
+        }
+        st.cur ^= 1;  // only the phase planes of the new set are meaningful here
+        const double rel = fabs(previous - new_energy) / fmax(fabs(previous), 1e-300);
+        steps = step;
+        energy_final = new_energy;
+        rel_final = rel;
+        change_final = actual_change;
+        previous = new_energy;
+        if (step >= min_steps && rel < energy_rtol && actual_change < 1e-5) {
+            converged = true;
+            break;
+        }
+    }
+    if (steps == 0) energy_final = e_init;
+    double e_after;
+    if (!phase_interface_energy(a, red, st.cur, e_after, frac)) return false;
+    rep[0] = steps;
+    rep[1] = converged ? 1 : 0;
+    rep[3] = energy_final;
+    rep[4] = rel_final;
+    rep[5] = change_final;
+    for (int k = 0; k < 3; ++k) rep[9 + k] = frac[k];
+    st.cache_valid = false;
+    return true;
+}
+
+// Sums of the mixture intercept and susceptibility (the mean_carbon solve of
+// initialize, pearl_serial.cpp:1814-1822).  Reduction: {sum c0, sum chi, invalid}.
+__device__ bool phase_mix_sums(const KArgs& a, Red& red, int s, double& si, double& sc, bool& mixbad) {
+    const DevParams& P = a.P;
+    const double* const* ph = a.B.phi[s];
+    double v0 = 0, v1 = 0, vb = 0;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            double chi, cint, K;
+            if (!mixture(P, ph[0][i], ph[1][i], ph[2][i], chi, cint, K)) vb = 1;
+            v0 += cint;
+            v1 += chi;
+        }
+    }
+    double v[3] = {v0, v1, vb};
+    if (!red.reduce<3>(v, OPS3(kSum, kSum, kMax), kTagInit)) return false;
+    si = v[0];
+    sc = v[1];
+    mixbad = v[2] != 0;
+    return true;
+}
+
+// Uniform mu and the carbon it implies (initialize, pearl_serial.cpp:1823-1826).
+// Reduction: {sum carbon, invalid}.
+__device__ bool phase_init_composition(const KArgs& a, Red& red, int s, double mu, double& mass, bool& mixbad) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const double* const* ph = B.phi[s];
+    double vm = 0, vb = 0;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            double chi, cint, K;
+            if (!mixture(P, ph[0][i], ph[1][i], ph[2][i], chi, cint, K)) vb = 1;
+            const double cc = fma(chi, mu, cint);
+            B.mu[s][i] = mu;
+            B.c[s][i] = cc;
+            vm += cc;
+        }
+    }
+    double v[2] = {vm, vb};
+    if (!red.reduce<2>(v, OPS2(kSum, kMax), kTagInit)) return false;
+    mass = v[0] * P.dx * P.dy;
+    mixbad = v[1] != 0;
+    return true;
+}
+
 // snapshot() reductions (pearl_serial.cpp:2266-2281) on state `s`.
 __device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
     const DevParams& P = a.P;
@@ -1115,6 +1396,41 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             ctl->out[5] = m;
             ctl->out[6] = e;
             ctl->iout[0] = mixbad;
+        }
+        red.flush();
+        return;
+    }
+    if (a.mode == kModeSmooth) {
+        double rep[12];
+        if (!smooth(a, red, st, rep)) return;
+        if (leader) {
+            for (int k = 0; k < 12; ++k) ctl->out[k] = rep[k];
+            ctl->cur = st.cur;
+            ctl->energy_valid = 0;
+        }
+        red.flush();
+        return;
+    }
+    if (a.mode == kModeMixSums) {
+        double si, sc;
+        bool mixbad;
+        if (!phase_mix_sums(a, red, st.cur, si, sc, mixbad)) return;
+        if (leader) {
+            ctl->out[0] = si;
+            ctl->out[1] = sc;
+            ctl->iout[0] = mixbad;
+        }
+        red.flush();
+        return;
+    }
+    if (a.mode == kModeInitComposition) {
+        double mass;
+        bool mixbad;
+        if (!phase_init_composition(a, red, st.cur, a.init_mu, mass, mixbad)) return;
+        if (leader) {
+            ctl->out[0] = mass;
+            ctl->iout[0] = mixbad;
+            ctl->energy_valid = 0;
         }
         red.flush();
         return;
@@ -1336,6 +1652,9 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
         case PEARL_ERR_MAX_STEPS: return fail(ctx, st, "configured max_steps reached before end_time");
         case PEARL_ERR_UNSAFE_SHIFT: return fail(ctx, st, "unsafe shift: removed strip contains gamma");
         case PEARL_ERR_NONFINITE_CARBON: return fail(ctx, st, "Nonfinite total carbon");
+        case PEARL_ERR_SMOOTHING:
+            return fail(ctx, st, ctx->h_ctl->why == 1 ? "nonfinite smoothing force"
+                                                      : "sharp smoothing could not find an energy-decreasing step");
         case PEARL_ERR_DEVICE_WAIT:
             // a grid barrier gave up waiting: reset the barrier words before any further launch
             ctx->h_ctl->bar_count = 0;
@@ -1428,6 +1747,7 @@ const char* pearl_gpu_status_string(int status) {
         case PEARL_ERR_NONFINITE_CARBON: return "Nonfinite total carbon";
         case PEARL_ERR_NO_DEVICE: return "no CUDA device";
         case PEARL_ERR_TOO_LARGE: return "domain exceeds the no-allocation scratch limit of 262144 cells";
+        case PEARL_ERR_SMOOTHING: return "sharp smoothing failed";
         default: return "unknown status";
     }
 }
@@ -1625,6 +1945,61 @@ int pearl_gpu_snapshot(pearl_gpu_ctx* ctx, pearl_diag* out) {
     out->mass = h->out[5];
     out->energy = h->out[6];
     out->ledger = out->mass + h->S.carbon_removed - h->S.carbon_added - h->S.initial_carbon;
+    return PEARL_OK;
+}
+
+int pearl_gpu_smooth_interface(pearl_gpu_ctx* ctx, int max_steps, int min_steps, double energy_rtol,
+                               double max_phase_change, pearl_smooth_report* out) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    // smooth_interface_only's control check (pearl_serial.cpp:874-876)
+    if (max_steps < 1 || min_steps < 0 || min_steps > max_steps || !(energy_rtol > 0) || !(max_phase_change > 0) ||
+        max_phase_change > .2)
+        return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid sharp-smoothing controls");
+    KArgs a{};
+    a.mode = kModeSmooth;
+    a.smooth_max_steps = max_steps;
+    a.smooth_min_steps = min_steps;
+    a.smooth_energy_rtol = energy_rtol;
+    a.smooth_max_phase_change = max_phase_change;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (out) {
+        const double* r = ctx->h_ctl->out;
+        out->steps = (int)r[0];
+        out->converged = (int)r[1];
+        out->energy_initial = r[2];
+        out->energy_final = r[3];
+        out->final_relative_energy_change = r[4];
+        out->final_max_phase_change = r[5];
+        for (int k = 0; k < 3; ++k) {
+            out->phase_fraction_before[k] = r[6 + k];
+            out->phase_fraction_after[k] = r[9 + k];
+        }
+    }
+    return PEARL_OK;
+}
+
+int pearl_gpu_mixture_sums(pearl_gpu_ctx* ctx, double* sum_c_intercept, double* sum_chi) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeMixSums;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
+    if (sum_c_intercept) *sum_c_intercept = ctx->h_ctl->out[0];
+    if (sum_chi) *sum_chi = ctx->h_ctl->out[1];
+    return PEARL_OK;
+}
+
+int pearl_gpu_init_composition(pearl_gpu_ctx* ctx, double mu, double* total_carbon) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    KArgs a{};
+    a.mode = kModeInitComposition;
+    a.init_mu = mu;
+    int rc = launch(ctx, a);
+    if (rc) return rc;
+    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
+    if (total_carbon) *total_carbon = ctx->h_ctl->out[0];
     return PEARL_OK;
 }
 

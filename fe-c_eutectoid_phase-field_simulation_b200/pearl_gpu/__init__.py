@@ -26,7 +26,7 @@ STATUS = {
     7: "Simplex projection failed", 8: "configured max_steps reached before end_time",
     9: "device wait limit exceeded", 10: "unsafe shift: removed strip contains gamma",
     11: "Nonfinite total carbon", 12: "no CUDA device",
-    13: "domain exceeds the no-allocation scratch limit of 262144 cells",
+    13: "domain exceeds the no-allocation scratch limit of 262144 cells", 14: "sharp smoothing failed",
 }
 
 
@@ -88,6 +88,12 @@ class PearlStepInfo(C.Structure):
     ]
 
 
+class PearlSmoothReport(C.Structure):
+    _fields_ = [("steps", C.c_int), ("converged", C.c_int), ("energy_initial", D), ("energy_final", D),
+                ("final_relative_energy_change", D), ("final_max_phase_change", D),
+                ("phase_fraction_before", D * 3), ("phase_fraction_after", D * 3)]
+
+
 class PearlRunLimits(C.Structure):
     _fields_ = [("max_steps", C.c_longlong), ("config_max_steps", C.c_longlong), ("stop_time", D),
                 ("end_time", D), ("output_eps", D)]
@@ -108,11 +114,12 @@ EXPORTS = [
     "pearl_gpu_maybe_shift", "pearl_gpu_snapshot", "pearl_gpu_propose_phi", "pearl_gpu_upload_trial_phi",
     "pearl_gpu_implicit_diffusion", "pearl_gpu_download_trial", "pearl_gpu_energy_mass", "pearl_gpu_valid_state",
     "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats", "pearl_gpu_phase_times",
-    "pearl_gpu_selftest_division", "pearl_gpu_advance_noalloc",
+    "pearl_gpu_selftest_division", "pearl_gpu_advance_noalloc", "pearl_gpu_smooth_interface",
+    "pearl_gpu_mixture_sums", "pearl_gpu_init_composition",
 ]
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
-          "mixture", "shift", "snapshot"]
+          "mixture", "shift", "snapshot", "smooth", "init"]
 
 _lib = None
 
@@ -153,6 +160,9 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
     L.pearl_gpu_phase_times.argtypes = [V, DP, C.POINTER(C.c_longlong)]
     L.pearl_gpu_selftest_division.argtypes = [C.c_int, DP, DP, C.c_longlong, C.POINTER(C.c_ulonglong)]
+    L.pearl_gpu_smooth_interface.argtypes = [V, C.c_int, C.c_int, D, D, C.POINTER(PearlSmoothReport)]
+    L.pearl_gpu_mixture_sums.argtypes = [V, DP, DP]
+    L.pearl_gpu_init_composition.argtypes = [V, D, DP]
     L.pearl_gpu_advance_noalloc.argtypes = [C.POINTER(PearlParams), C.c_int, C.c_int, V, V, V,
                                             C.POINTER(PearlScalars), D, C.POINTER(PearlStepInfo), V]
     if path is None:
@@ -266,6 +276,24 @@ class Context:
         d = PearlDiag()
         self._check(self.lib.pearl_gpu_snapshot(self.h, C.byref(d)))
         return d
+
+    # ---- initialisation (pearl::initialize)
+    def smooth_interface(self, max_steps: int = 100, min_steps: int = 100, energy_rtol: float = 1e-10,
+                         max_phase_change: float = 0.02) -> PearlSmoothReport:
+        rep = PearlSmoothReport()
+        self._check(self.lib.pearl_gpu_smooth_interface(self.h, max_steps, min_steps, energy_rtol, max_phase_change,
+                                                        C.byref(rep)))
+        return rep
+
+    def mixture_sums(self):
+        a, b = D(), D()
+        self._check(self.lib.pearl_gpu_mixture_sums(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def init_composition(self, mu: float) -> float:
+        m = D()
+        self._check(self.lib.pearl_gpu_init_composition(self.h, mu, C.byref(m)))
+        return m.value
 
     # ---- single functions of the hot path
     def propose_phi(self, dt: float) -> float:

@@ -27,7 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = {
     "pearl_fp64.cu": ["-fmad=false"],
 }
-HOST_SOURCES: list[str] = []
+# host driver (the pearl_gpu executable): C++17, linked against libpearl_gpu.so
+CLI_SOURCES = ["config.cpp", "io.cpp", "main.cpp"]
 
 
 def _run(cmd: list[str]) -> None:
@@ -60,12 +61,13 @@ def build(force: bool = False, verbose: bool = False) -> Path:
                 cmd.insert(1, "-Xptxas=-v")
             _run(cmd)
             objs.append(obj)
-        for name in HOST_SOURCES:
-            obj = BUILD / (Path(name).stem + ".host.o")
-            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{HOST}",
-                  "-c", str(HOST / name), "-o", str(obj)])
-            objs.append(obj)
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(LIB)])
+    if force or _newer(CLI, deps + [LIB]):
+        # -ffp-contract=off: host arithmetic that mirrors the reference (temperature
+        # laws, initial geometry) is rounded operation by operation like it
+        _run(["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{HOST}",
+              *[str(HOST / n) for n in CLI_SOURCES], f"-L{BUILD}", "-lpearl_gpu", "-Wl,-rpath,$ORIGIN",
+              "-o", str(CLI)])
     return LIB
 
 

@@ -103,7 +103,9 @@ typedef enum pearl_status {
     PEARL_ERR_UNSAFE_SHIFT = 10,          /* "unsafe shift: removed strip contains gamma" (:2068) */
     PEARL_ERR_NONFINITE_CARBON = 11,      /* "Nonfinite total carbon" (:140) */
     PEARL_ERR_NO_DEVICE = 12,
-    PEARL_ERR_TOO_LARGE = 13              /* domain exceeds the no-allocation scratch (no reference counterpart) */
+    PEARL_ERR_TOO_LARGE = 13,             /* domain exceeds the no-allocation scratch (no reference counterpart) */
+    PEARL_ERR_SMOOTHING = 14              /* "nonfinite smoothing force" (:920) or
+                                             "sharp smoothing could not find an energy-decreasing step" (:940) */
 } pearl_status;
 
 /* Rejection reason <why> of the last attempt (pearl_serial.cpp:1133-1160). */
@@ -115,6 +117,13 @@ typedef enum pearl_why {
     PEARL_WHY_MASS = 4,             /* "mass conservation" */
     PEARL_WHY_ENERGY = 5            /* "free-energy increase" */
 } pearl_why;
+
+/* pearl::SmoothReport (pearl_serial.cpp:844-853). */
+typedef struct pearl_smooth_report {
+    int steps, converged;
+    double energy_initial, energy_final, final_relative_energy_change, final_max_phase_change;
+    double phase_fraction_before[3], phase_fraction_after[3];
+} pearl_smooth_report;
 
 typedef struct pearl_gpu_ctx pearl_gpu_ctx;
 
@@ -154,6 +163,18 @@ int pearl_gpu_maybe_shift(pearl_gpu_ctx* ctx, double shift_trigger, double shift
 
 /* Output-time reductions of snapshot() (pearl_serial.cpp:2266-2281). */
 int pearl_gpu_snapshot(pearl_gpu_ctx* ctx, pearl_diag* out);
+
+/* ---- initialisation on the device (pearl::initialize, pearl_serial.cpp:1761-1837) ---- */
+/* Capillarity-only smoothing of the current phase fields
+ * (smooth_interface_only, pearl_serial.cpp:869-958). */
+int pearl_gpu_smooth_interface(pearl_gpu_ctx* ctx, int max_steps, int min_steps, double energy_rtol,
+                               double max_phase_change, pearl_smooth_report* out);
+/* Sums over cells of mixture(phi).c_intercept and .susceptibility: the
+ * mean_carbon chemical-potential solve (pearl_serial.cpp:1814-1822). */
+int pearl_gpu_mixture_sums(pearl_gpu_ctx* ctx, double* sum_c_intercept, double* sum_chi);
+/* mu = `mu` everywhere and carbon = composition(mu, mixture(phi))
+ * (pearl_serial.cpp:1823-1826); *total_carbon receives total_carbon (:784-788). */
+int pearl_gpu_init_composition(pearl_gpu_ctx* ctx, double mu, double* total_carbon);
 
 /* ---- single hot-path functions, for per-function parity checks ---- */
 /* propose_phi (pearl_serial.cpp:961-1002): writes the proposal into the trial buffer. */
