@@ -218,8 +218,28 @@ int main(int argc, char** argv) {
             }
             double mu = config.initial_mu;
             if (config.composition_mode == "mean") {
+                // One-time solve of pearl_serial.cpp:1814-1822.  Its two sums cancel
+                // strongly, so they are formed on the host in the reference's
+                // sequential order, which makes mu_reference bitwise equal to it.
+                if (config.initialization == "sharp_smooth" || config.initialization == "microsim") {
+                    // st.phi already holds the smoothed fields
+                } else {
+                    gpu.check(pearl_gpu_download(gpu.ctx, st.phi.data(), nullptr, nullptr, nullptr));
+                }
                 double si = 0, sc = 0;
-                gpu.check(pearl_gpu_mixture_sums(gpu.ctx, &si, &sc));
+                for (size_t i = 0; i < cells; ++i) {
+                    const auto p = cell_phi(st.phi, i);
+                    const double triple = 2.0 * p[0] * p[1] * p[2];
+                    double chi = 0.0, ci = 0.0;
+                    for (int q = 0; q < 3; ++q) {
+                        const double h = p[q] * p[q] * (3.0 - 2.0 * p[q]) + triple;
+                        const double cq = config.thermo[q].chi();
+                        chi += h * cq;
+                        ci -= h * cq * config.thermo[q].B;
+                    }
+                    si += ci;
+                    sc += chi;
+                }
                 mu = (config.nx * config.ny * config.initial_carbon - si) / sc;
             }
             double mass = 0;

@@ -90,11 +90,15 @@ def test_cli_run_matches_reference(cli, golden, tmp_path, name):
     head, rows = _csv((out / "diagnostics.csv").read_text())
     rhead, rrows = _csv(ref["diagnostics"])
     assert head == rhead and len(rows) == len(rrows)
+    kv = dict(cli_inputs.VALID[name]())
+    area = int(kv["nx"]) * int(kv["ny"]) * float(kv["dx"]) ** 2
     for r, g in zip(rows, rrows):
         for k in ("time", "step", "dt_next", "cg_last", "cg_peak", "rejected", "shift_distance"):
             assert r[k] == g[k], k
         assert r["mean_carbon"] == pytest.approx(g["mean_carbon"], rel=1e-13)
-        assert abs(r["mass_ledger_error"] - g["mass_ledger_error"]) <= 1e-12 * g["mean_carbon"] * 1e-16
+        # the ledger is rounding noise of the total carbon: compare on that scale
+        total = g["mean_carbon"] * area
+        assert abs(r["mass_ledger_error"] - g["mass_ledger_error"]) <= 1e-13 * total
         assert r["reduced_energy"] == pytest.approx(g["reduced_energy"], rel=1e-10)
         assert abs(r["phi_sum_error"] - g["phi_sum_error"]) <= 1e-15
         for k in ("c_min", "c_max"):
