@@ -155,6 +155,24 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def reduce_over_ranks(dist, x: float, op: str, device: str) -> float:
+    """Max or sum of a per-rank scalar (replicas: throughput is the sum of cells over the
+    slowest rank's time).  Identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_throughput(dist, cells: float, seconds: float, device: str) -> tuple[float, float]:
+    """(whole-job cell-updates/s, max time over ranks) for independent replicas."""
+    t_max = reduce_over_ranks(dist, seconds, "max", device)
+    return reduce_over_ranks(dist, cells, "sum", device) / t_max, t_max
+
+
 # ------------------------------------------------------------------ CPU sides
 def cpu_sample(w, seconds: float, max_steps: int | None = None):
     """Time the reference (or the C restatement) on one host core over whole steps of the
@@ -249,18 +267,10 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_over_ranks(dist, x, "max", "cuda")
 
     def sum_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+        return reduce_over_ranks(dist, x, "sum", "cuda")
 
     # warm-up (also fills the step-energy cache)
     ctx.run(max(args.warmup, 1))
@@ -285,9 +295,7 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
     rejected = ctx.scalars().rejected - rejected0
     elapsed = ev0.elapsed_time(ev1) / 1e3
     assert rep.steps == args.steps, "run stopped early"
-    t_max = max_over_ranks(elapsed)
-    cells_total = sum_over_ranks(float(w.cells * rep.steps))
-    value = cells_total / t_max
+    value, t_max = replica_throughput(dist, float(w.cells * rep.steps), elapsed, "cuda")
 
     # roofline of the persistent kernel: algorithmic bytes of its launch over its event time
     algo_bytes = w.cells * (80.0 * rep.steps + 64.0 * rep.cg_total)
