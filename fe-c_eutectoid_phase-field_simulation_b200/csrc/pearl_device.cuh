@@ -9,6 +9,7 @@
 // sequential row-major loop.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -27,6 +28,7 @@ constexpr int kMaxRed = 6;  // values per grid reduction
 // equal what the reference recomputes per cell.
 struct DevParams {
     int nx, ny, pitch, ntx, nty, ntiles;
+    int warps_x_log2;  // tile = (32 << warps_x_log2) x (2 << (3 - warps_x_log2)) cells
     double dx, dy, dx2, dy2;
     double Vm, eps, obs, tr, two_eps_sigma, eps_sigma;
     double tau[3], tau_min;
@@ -82,6 +84,8 @@ struct DevBufs {
     double* z;
     double* p[2];  // search direction, double-buffered (read at neighbours while rewritten)
     double* Ap;
+    double* wE;    // east-face weight .5*(K+K_east)/dx^2 of the current solve
+    double* wN;    // north-face weight .5*(K+K_north)/dy^2, zero at the top wall
     double* part;  // [2][grid][kMaxRed] block partials
     struct Ctl* ctl;
 };
@@ -177,6 +181,60 @@ __device__ __forceinline__ double local_tau(const DevParams& P, double p0, doubl
     const double w0 = p0 * p1, w1 = p0 * p2, w2 = p1 * p2;
     const double s = w0 + w1 + w2;
     return s > 1e-30 ? (w0 * P.tau[0] + w1 * P.tau[1] + w2 * P.tau[2]) / s : P.tau_min;
+}
+
+// ---------------------------------------------------------------- TMA tile staging
+// A 32x16-cell tile plus a one-cell halo is staged per field as one 2-D TMA
+// box.  The box starts two cells left of the tile so that its x coordinate
+// stays a multiple of two doubles (16 bytes): columns 0..35 hold x0-2..x0+33,
+// rows 0..17 hold y0-1..y0+16.  Out-of-range rows and columns arrive as zeros;
+// the periodic x wrap is patched with plain loads and the y walls never read
+// their ghost row (the zero-flux faces are skipped or weighted by zero).
+constexpr int kBoxW = kTileX + 4;
+constexpr int kBoxH = kTileRows + 2;
+constexpr uint32_t kBoxBytes = kBoxW * kBoxH * sizeof(double);        // 5184
+constexpr int kFieldStride = ((kBoxBytes + 127) / 128 * 128) / 8;     // doubles per staged field (128 B aligned)
+constexpr int kMaxStageFields = 8;
+constexpr int kMaxStages = 4;
+// Shared-memory budget of the pipeline: two stages of the widest phase (8 fields);
+// phases staging fewer fields run more stages in the same space (up to 4).
+constexpr size_t kPipeDoubles = (size_t)2 * kMaxStageFields * kFieldStride;
+constexpr size_t kTmaSmemBytes = 128 + kPipeDoubles * sizeof(double);
+
+// Tensor-map slots: state set s fields 0..4 (phi_a, phi_t, phi_g, c, mu) at
+// 5*s + f, then the work planes.
+enum MapId : int {
+    kMapState = 0,  // + 5*set + field
+    kMapK = 10, kMapChi, kMapIcpt, kMapX, kMapZ, kMapP0, kMapP1, kMapWE, kMapWN, kMapCount
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Generic-proxy writes (plain stores) made visible to later TMA (async-proxy) reads.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // ---------------------------------------------------------------- grid barrier

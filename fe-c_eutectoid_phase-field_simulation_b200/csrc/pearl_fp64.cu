@@ -23,10 +23,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <cudaTypedefs.h>
 
 #include "pearl_device.cuh"
 #include "pearl_gpu.h"
@@ -48,6 +51,8 @@ enum Mode : int {
 };
 
 struct KArgs {
+    CUtensorMap maps[kMapCount];  // 2-D TMA descriptors of the staged planes (valid when use_tma)
+    int use_tma;
     DevParams P;
     DevBufs B;
     int mode;
@@ -71,8 +76,11 @@ struct Pair {
 __device__ __forceinline__ Pair pair_of(const DevParams& P, int t) {
     Pair c;
     const int bx = t % P.ntx, by = t / P.ntx;
-    c.x = bx * kTileX + (threadIdx.x & 31);
-    c.y0 = by * kTileRows + 2 * (threadIdx.x >> 5);
+    // the 8 warps of a block are arranged 2^wx side by side in x and 8/2^wx in y
+    const int warp = threadIdx.x >> 5;
+    const int wx = warp & ((1 << P.warps_x_log2) - 1), wy = warp >> P.warps_x_log2;
+    c.x = (bx << (5 + P.warps_x_log2)) + (wx << 5) + (threadIdx.x & 31);
+    c.y0 = (by << (4 - P.warps_x_log2)) + 2 * wy;
     c.v0 = c.x < P.nx && c.y0 < P.ny;
     c.v1 = c.v0 && c.y0 + 1 < P.ny;
     const int xw = c.x == 0 ? P.nx - 1 : c.x - 1;
@@ -237,6 +245,7 @@ struct Red {
     const KArgs& a;
     PhaseClock* clk;  // shared memory; used by thread 0 of block 0 only
     unsigned counter = 0;
+    struct Pipe* pipe_ptr = nullptr;
     __device__ Red(const KArgs& args, PhaseClock* c) : a(args), clk(c) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             clk->t_last = globaltimer_ns();
@@ -249,6 +258,8 @@ struct Red {
     // publish the block partials, wait for the grid, combine; false on a device-wait timeout
     template <int NV>
     __device__ bool reduce(double (&v)[NV], unsigned ops, int tag) {
+        // this thread's plane stores may be read by TMA (async proxy) after the barrier
+        if (a.use_tma) fence_proxy_async();
         double* slot = a.B.part + (size_t)(counter & 1u) * gridDim.x * kMaxRed;
         ++counter;
         block_publish<NV>(v, ops, slot);
@@ -278,16 +289,181 @@ struct Red {
 
 #define FOR_TILES(P) for (int t = blockIdx.x; t < (P).ntiles; t += gridDim.x)
 
+// ------------------------------------------------------------------ stencil sources
+// A phase body reads its input fields through a source that maps a field slot
+// and a neighbour of one of the thread's two cells to a value.  GlobalSrc
+// reads the planes directly; SmemSrc reads the tile staged by TMA.  The body,
+// and therefore the arithmetic, is the same for both.
+enum Dir : int { kC = 0, kW = 1, kE = 2, kS = 3, kN = 4 };
+
+template <int NF>
+struct GlobalSrc {
+    const double* f[NF];
+    Pair c;
+    __device__ __forceinline__ double v(int k, int cell, int dir) const {
+        size_t i;
+        if (cell == 0)
+            i = dir == kC ? c.i0 : dir == kW ? c.iw0 : dir == kE ? c.ie0 : dir == kS ? c.is0 : (c.v1 ? c.i1 : c.i0);
+        else
+            i = dir == kC ? c.i1 : dir == kW ? c.iw1 : dir == kE ? c.ie1 : dir == kS ? c.i0 : c.in1;
+        return f[k < NF ? k : 0][i];
+    }
+};
+
+template <int NF>
+struct SmemSrc {
+    const double* base;  // stage base: field k at base + k*kFieldStride
+    int lx, ly0;         // box column of x, box row of the lower cell
+    bool south, v1, north1;
+    __device__ __forceinline__ double v(int k, int cell, int dir) const {
+        int ly = ly0 + cell, x = lx;
+        if (dir == kW) x -= 1;
+        if (dir == kE) x += 1;
+        if (dir == kS) ly = cell == 0 ? (south ? ly - 1 : ly) : ly - 1;
+        if (dir == kN) ly = cell == 0 ? (v1 ? ly + 1 : ly) : (north1 ? ly + 1 : ly);
+        return base[k * kFieldStride + ly * kBoxW + x];
+    }
+};
+
+// Both cells' five-point stencils of slot k (see S2); the upper cell's own
+// neighbours are only read when it is inside the domain.
+template <class Src>
+__device__ __forceinline__ S2 stencil2(const Src& s, int k, bool v1) {
+    S2 r;
+    r.c0 = s.v(k, 0, kC);
+    r.w0 = s.v(k, 0, kW);
+    r.e0 = s.v(k, 0, kE);
+    r.s0 = s.v(k, 0, kS);
+    r.c1 = s.v(k, 0, kN);  // upper cell, or the lower cell itself at the top wall
+    if (v1) {
+        r.w1 = s.v(k, 1, kW);
+        r.e1 = s.v(k, 1, kE);
+        r.n1 = s.v(k, 1, kN);
+    } else {
+        r.w1 = r.e1 = r.n1 = 0;
+    }
+    return r;
+}
+
+// Face weights of cell `cell` of the pair from the stored east/north faces of
+// this solve: the west face is the west neighbour's east face and the south
+// face the south neighbour's north face (IEEE addition is commutative, so
+// these equal weights_at's recomputation bitwise); zero at the walls.
+template <class Src>
+__device__ __forceinline__ Faces faces_stored(const Src& src, int se, int sn, int cell, const Pair& c) {
+    Faces f;
+    f.w0 = src.v(se, cell, kW);
+    f.w1 = src.v(se, cell, kC);
+    f.w2 = cell == 0 ? (c.y0 == 0 ? 0.0 : src.v(sn, 0, kS)) : src.v(sn, 0, kC);
+    f.w3 = src.v(sn, cell, kC);
+    return f;
+}
+
+// ------------------------------------------------------------------ TMA pipeline
+struct Pipe {
+    uint64_t* bar;     // kMaxStages mbarriers in shared memory
+    double* stage;     // stage buffers (kPipeDoubles)
+    uint32_t parity;   // bit s: next completion phase expected on barrier s
+};
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned it = 1;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63u) == 0 && globaltimer_ns() - t0 > kBarrierTimeoutNs) return false;
+    }
+}
+
+// Sweep the block's tiles, calling body(src, pair) for every tile whose first
+// cell is inside the domain.  With TMA, field slot k of tile t is staged from
+// tensor map maps[k]; slots whose bit is set in `stencil` also get the
+// periodic x wrap patched from `planes`.  Returns false after a bounded wait
+// ran out (the status is recorded; in-flight copies are drained, bounded).
+template <int NF, class Body>
+__device__ bool sweep(const KArgs& a, Pipe& pp, const int (&maps)[NF], const double* const (&planes)[NF],
+                      unsigned stencil, Body&& body) {
+    const DevParams& P = a.P;
+    if (!a.use_tma) {
+        FOR_TILES(P) {
+            const Pair c = pair_of(P, t);
+            if (!c.v0) continue;
+            GlobalSrc<NF> src;
+#pragma unroll
+            for (int k = 0; k < NF; ++k) src.f[k] = planes[k];
+            src.c = c;
+            body(src, c);
+        }
+        return true;
+    }
+    constexpr int S = (int)(kPipeDoubles / ((size_t)NF * kFieldStride)) < kMaxStages
+                          ? (int)(kPipeDoubles / ((size_t)NF * kFieldStride))
+                          : kMaxStages;
+    static_assert(S >= 2, "pipeline needs two stages");
+    const int G = gridDim.x;
+    const int nb = (int)blockIdx.x < P.ntiles ? (P.ntiles - 1 - (int)blockIdx.x) / G + 1 : 0;
+    const auto issue = [&](int k) {
+        if (threadIdx.x != 0) return;
+        const int t = blockIdx.x + k * G;
+        const int bx = t % P.ntx, by = t / P.ntx;
+        const int s = k % S;
+        double* dst = pp.stage + (size_t)s * NF * kFieldStride;
+        fence_proxy_async();  // earlier plain stores (global, and the stage's patch) before these async reads/writes
+        mbar_arrive_expect_tx(&pp.bar[s], NF * kBoxBytes);
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+            tma_load_2d(dst + f * kFieldStride, &a.maps[maps[f]], bx * kTileX - 2, by * kTileRows - 1, &pp.bar[s]);
+    };
+    for (int k = 0; k < S - 1 && k < nb; ++k) issue(k);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < nb; ++k) {
+        const int s = k % S;
+        if (k + S - 1 < nb) issue(k + S - 1);
+        if (!mbar_wait_bounded(&pp.bar[s], (pp.parity >> s) & 1u)) {
+            atomicCAS(&a.B.ctl->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
+            for (int j = k + 1; j < nb && j < k + S; ++j)  // drain the copies still in flight, bounded
+                mbar_wait_bounded(&pp.bar[j % S], (pp.parity >> (j % S)) & 1u);
+            return false;
+        }
+        pp.parity ^= 1u << s;
+        const int t = blockIdx.x + k * G;
+        const int bx = t % P.ntx, by = t / P.ntx;
+        double* st = pp.stage + (size_t)s * NF * kFieldStride;
+        const bool left = bx == 0, right = (bx + 1) * kTileX >= P.nx;
+        if (left || right) {
+            // periodic wrap: box column of x=-1 from x=nx-1, box column of x=nx from x=0
+            for (int idx = threadIdx.x; idx < NF * 2 * kBoxH; idx += kThreads) {
+                const int f = idx / (2 * kBoxH), side = (idx / kBoxH) & 1, r = idx % kBoxH;
+                if (!((stencil >> f) & 1u) || (side == 0 && !left) || (side == 1 && !right)) continue;
+                int y = by * kTileRows - 1 + r;
+                y = y < 0 ? 0 : (y > P.ny - 1 ? P.ny - 1 : y);
+                const int col = side == 0 ? 1 : P.nx - (bx * kTileX - 2);
+                st[f * kFieldStride + r * kBoxW + col] = planes[f][(size_t)y * P.pitch + (side == 0 ? P.nx - 1 : 0)];
+            }
+            __syncthreads();
+        }
+        const Pair c = pair_of(P, t);
+        if (c.v0) {
+            SmemSrc<NF> src{st, lane + 2, 2 * warp + 1, c.y0 > 0, c.v1, c.y0 + 2 < P.ny};
+            body(src, c);
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
 // ------------------------------------------------------------------ phases
-// propose_phi for one cell (pearl_serial.cpp:966-1001); returns the trial phi.
+// propose_phi for cell `k` of the pair (pearl_serial.cpp:966-1001); slots 0-2
+// hold phi, slot 3 holds mu.
 struct Proposal {
     double z0, z1, z2, change;
     bool simplex_bad;
 };
-__device__ __forceinline__ Proposal propose_cell(const DevParams& P, const double* const* ph, double mu, double dt,
-                                                 size_t i, size_t iw, size_t ie, size_t is, size_t in, bool south,
+template <class Src>
+__device__ __forceinline__ Proposal propose_cell(const DevParams& P, const Src& src, int k, double dt, bool south,
                                                  bool north) {
-    const double q0 = ph[0][i], q1 = ph[1][i], q2 = ph[2][i];
+    const double q0 = src.v(0, k, kC), q1 = src.v(1, k, kC), q2 = src.v(2, k, kC);
+    const double mu = src.v(3, k, kC);
     const double psi0 = psi(P, 2, mu);
     const double ps[3] = {psi(P, 0, mu), psi(P, 1, mu), psi0};
     const double q[3] = {q0, q1, q2};
@@ -307,8 +483,8 @@ __device__ __forceinline__ Proposal propose_cell(const DevParams& P, const doubl
 #pragma unroll
     for (int dir = 0; dir < 4; ++dir) {
         if ((dir == 2 && !south) || (dir == 3 && !north)) continue;
-        const size_t j = dir == 0 ? iw : (dir == 1 ? ie : (dir == 2 ? is : in));
-        const double n[3] = {ph[0][j], ph[1][j], ph[2][j]};
+        const int d = dir == 0 ? kW : dir == 1 ? kE : dir == 2 ? kS : kN;
+        const double n[3] = {src.v(0, k, d), src.v(1, k, d), src.v(2, k, d)};
         const double d2 = dir < 2 ? P.dx2 : P.dy2, rd2 = dir < 2 ? P.r_dx2 : P.r_dy2;
 #pragma unroll
         for (int aa = 0; aa < 3; ++aa)
@@ -346,23 +522,22 @@ __device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, doub
                               bool& simplexbad) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    const double* const* ph = B.phi[cur];
     double* const* tp = B.phi[cur ^ 1];
     double vchange = 0, vmix = 0, vsimp = 0;
-    FOR_TILES(P) {
-        const Pair c = pair_of(P, t);
-        if (!c.v0) continue;
+    const int maps[4] = {kMapState + 5 * cur, kMapState + 5 * cur + 1, kMapState + 5 * cur + 2,
+                         kMapState + 5 * cur + 4};
+    const double* const planes[4] = {B.phi[cur][0], B.phi[cur][1], B.phi[cur][2], B.mu[cur]};
+    const bool ok = sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, [&](const auto& src, const Pair& c) {
 #pragma unroll 1
         for (int k = 0; k < 2; ++k) {
             if (k == 1 && !c.v1) break;
             const int y = c.y0 + k;
             const size_t i = k ? c.i1 : c.i0;
-            const size_t iw = k ? c.iw1 : c.iw0, ie = k ? c.ie1 : c.ie0;
-            const size_t is = k ? c.i0 : c.is0, in = k ? c.in1 : c.i1;
-            const double mu = B.mu[cur][i];
-            const Proposal o = propose_cell(P, ph, mu, dt, i, iw, ie, is, in, y > 0, y < P.ny - 1);
-            if (o.change == INFINITY) vchange = INFINITY;
-            else vchange = fmax(vchange, o.change);
+            const Proposal o = propose_cell(P, src, k, dt, y > 0, y < P.ny - 1);
+            if (o.change == INFINITY)
+                vchange = INFINITY;
+            else
+                vchange = fmax(vchange, o.change);
             if (o.simplex_bad) vsimp = 1;
             tp[0][i] = o.z0;
             tp[1][i] = o.z1;
@@ -373,11 +548,13 @@ __device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, doub
             B.chi[i] = chi;
             B.icpt[i] = fma(chi, P.mu_ref, cint);
             if (P.phase_only) {
+                const double mu = src.v(3, k, kC);
                 B.c[cur ^ 1][i] = fma(chi, mu, cint);
                 B.mu[cur ^ 1][i] = mu;
             }
         }
-    }
+    });
+    if (!ok) return false;
     double v[3] = {vchange, vmix, vsimp};
     if (!red.reduce<3>(v, OPS3(kMax, kMax, kMax), kTagPropose)) return false;
     change = v[0];
@@ -411,32 +588,28 @@ __device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
 }
 
 // SETUP: apply(mu_offset) and the initial residual (pearl_serial.cpp:1036-1046).
-// Reduction: {<rhs,rhs>, <r,z>, <r,r>}.
+// Slots: K, mu (stencils), chi, icpt, c.  Reduction: {<rhs,rhs>, <r,z>, <r,r>}.
 __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double& rhs2, double& rz, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double s0 = 0, s1 = 0, s2 = 0;
-    FOR_TILES(P) {
-        const Pair c = pair_of(P, t);
-        if (!c.v0) continue;
-        const S2 K = load_s2(B.K, c);
-        S2 u = load_s2(B.mu[cur], c);
-        const double chi0 = B.chi[c.i0], ic0 = B.icpt[c.i0], cold0 = B.c[cur][c.i0];
-        double chi1 = 0, ic1 = 0, cold1 = 0;
-        if (c.v1) {
-            chi1 = B.chi[c.i1];
-            ic1 = B.icpt[c.i1];
-            cold1 = B.c[cur][c.i1];
-        }
+    const int maps[5] = {kMapK, kMapState + 5 * cur + 4, kMapChi, kMapIcpt, kMapState + 5 * cur + 3};
+    const double* const planes[5] = {B.K, B.mu[cur], B.chi, B.icpt, B.c[cur]};
+    const bool ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x3u, [&](const auto& src, const Pair& c) {
+        const S2 K = stencil2(src, 0, c.v1);
+        S2 u = stencil2(src, 1, c.v1);
         u.c0 -= P.mu_ref; u.c1 -= P.mu_ref; u.w0 -= P.mu_ref; u.e0 -= P.mu_ref;
         u.w1 -= P.mu_ref; u.e1 -= P.mu_ref; u.s0 -= P.mu_ref; u.n1 -= P.mu_ref;
         {
+            const double chi = src.v(2, 0, kC), ic = src.v(3, 0, kC), cold = src.v(4, 0, kC);
             const Faces f = faces0(P, K, c);
-            const double Au = apply0(chi0, dt, f, u);
-            const double diag = chi0 + dt * (f.w0 + f.w1 + f.w2 + f.w3);
-            const double rhs = cold0 - ic0;
+            const double Au = apply0(chi, dt, f, u);
+            const double diag = chi + dt * (f.w0 + f.w1 + f.w2 + f.w3);
+            const double rhs = cold - ic;
             const double r = rhs - Au;
             const double z = r / diag;
+            B.wE[c.i0] = f.w1;
+            B.wN[c.i0] = f.w3;
             B.x[c.i0] = u.c0;
             B.r[c.i0] = r;
             B.z[c.i0] = z;
@@ -446,12 +619,15 @@ __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double
             s2 += r * r;
         }
         if (c.v1) {
+            const double chi = src.v(2, 1, kC), ic = src.v(3, 1, kC), cold = src.v(4, 1, kC);
             const Faces f = faces1(P, K, c);
-            const double Au = apply1(chi1, dt, f, u);
-            const double diag = chi1 + dt * (f.w0 + f.w1 + f.w2 + f.w3);
-            const double rhs = cold1 - ic1;
+            const double Au = apply1(chi, dt, f, u);
+            const double diag = chi + dt * (f.w0 + f.w1 + f.w2 + f.w3);
+            const double rhs = cold - ic;
             const double r = rhs - Au;
             const double z = r / diag;
+            B.wE[c.i1] = f.w1;
+            B.wN[c.i1] = f.w3;
             B.x[c.i1] = u.c1;
             B.r[c.i1] = r;
             B.z[c.i1] = z;
@@ -460,7 +636,8 @@ __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double
             s1 += r * z;
             s2 += r * r;
         }
-    }
+    });
+    if (!ok) return false;
     double v[3] = {s0, s1, s2};
     if (!red.reduce<3>(v, OPS3(kSum, kSum, kSum), kTagSetup)) return false;
     rhs2 = v[0];
@@ -470,18 +647,15 @@ __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double
 }
 
 // APPLY: p_new = z (first) or z + beta*p_old, written to p[pout]; Ap; <p,Ap>.
+// Slots: wE, wN, z (stencils), chi, p_old (stencil).
 __device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
-    const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double* pn = B.p[pout];
     double s = 0;
-    FOR_TILES(P) {
-        const Pair c = pair_of(P, t);
-        if (!c.v0) continue;
-        const S2 K = load_s2(B.K, c);
-        S2 p = load_s2(B.z, c);
+    const auto body = [&](const auto& src, const Pair& c) {
+        S2 p = stencil2(src, 2, c.v1);
         if (!first) {
-            const S2 po = load_s2(B.p[pout ^ 1], c);
+            const S2 po = stencil2(src, 4, c.v1);
             p.c0 = p.c0 + beta * po.c0;
             p.c1 = p.c1 + beta * po.c1;
             p.w0 = p.w0 + beta * po.w0;
@@ -491,19 +665,28 @@ __device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, dou
             p.s0 = p.s0 + beta * po.s0;
             p.n1 = p.n1 + beta * po.n1;
         }
-        const double chi0 = B.chi[c.i0];
-        const double chi1 = c.v1 ? B.chi[c.i1] : 0.0;
-        const double Ap0 = apply0(chi0, dt, faces0(P, K, c), p);
+        const double Ap0 = apply0(src.v(3, 0, kC), dt, faces_stored(src, 0, 1, 0, c), p);
         pn[c.i0] = p.c0;
         B.Ap[c.i0] = Ap0;
         s += p.c0 * Ap0;
         if (c.v1) {
-            const double Ap1 = apply1(chi1, dt, faces1(P, K, c), p);
+            const double Ap1 = apply1(src.v(3, 1, kC), dt, faces_stored(src, 0, 1, 1, c), p);
             pn[c.i1] = p.c1;
             B.Ap[c.i1] = Ap1;
             s += p.c1 * Ap1;
         }
+    };
+    bool ok;
+    if (first) {
+        const int maps[4] = {kMapWE, kMapWN, kMapZ, kMapChi};
+        const double* const planes[4] = {B.wE, B.wN, B.z, B.chi};
+        ok = sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, body);
+    } else {
+        const int maps[5] = {kMapWE, kMapWN, kMapZ, kMapChi, pout ? kMapP0 : kMapP1};
+        const double* const planes[5] = {B.wE, B.wN, B.z, B.chi, B.p[pout ^ 1]};
+        ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x17u, body);
     }
+    if (!ok) return false;
     double v[1] = {s};
     if (!red.reduce<1>(v, kSum, kTagApply)) return false;
     pAp = v[0];
@@ -553,33 +736,28 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
 }
 
 // TRUE_RES: r = rhs - A x; <r,r>  (pearl_serial.cpp:1051-1055)
+// Slots: wE, wN, x (stencils), chi, icpt, c.
 __device__ bool phase_true_residual(const KArgs& a, Red& red, int cur, double dt, double& rr) {
-    const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double s = 0;
-    FOR_TILES(P) {
-        const Pair c = pair_of(P, t);
-        if (!c.v0) continue;
-        const S2 K = load_s2(B.K, c);
-        const S2 x = load_s2(B.x, c);
-        const double chi0 = B.chi[c.i0], ic0 = B.icpt[c.i0], c0 = B.c[cur][c.i0];
-        double chi1 = 0, ic1 = 0, c1 = 0;
-        if (c.v1) {
-            chi1 = B.chi[c.i1];
-            ic1 = B.icpt[c.i1];
-            c1 = B.c[cur][c.i1];
-        }
+    const int maps[6] = {kMapWE, kMapWN, kMapX, kMapChi, kMapIcpt, kMapState + 5 * cur + 3};
+    const double* const planes[6] = {B.wE, B.wN, B.x, B.chi, B.icpt, B.c[cur]};
+    const bool ok = sweep<6>(a, *red.pipe_ptr, maps, planes, 0x7u, [&](const auto& src, const Pair& c) {
+        const S2 x = stencil2(src, 2, c.v1);
         {
-            const double r = (c0 - ic0) - apply0(chi0, dt, faces0(P, K, c), x);
+            const double r = (src.v(5, 0, kC) - src.v(4, 0, kC)) -
+                             apply0(src.v(3, 0, kC), dt, faces_stored(src, 0, 1, 0, c), x);
             B.r[c.i0] = r;
             s += r * r;
         }
         if (c.v1) {
-            const double r = (c1 - ic1) - apply1(chi1, dt, faces1(P, K, c), x);
+            const double r = (src.v(5, 1, kC) - src.v(4, 1, kC)) -
+                             apply1(src.v(3, 1, kC), dt, faces_stored(src, 0, 1, 1, c), x);
             B.r[c.i1] = r;
             s += r * r;
         }
-    }
+    });
+    if (!ok) return false;
     double v[1] = {s};
     if (!red.reduce<1>(v, kSum, kTagTrueRes)) return false;
     rr = v[0];
@@ -611,50 +789,49 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
 // FINAL: carbon update, closure and mu (pearl_serial.cpp:1082-1093) fused with
 // valid_state, total_carbon and reduced_energy of the trial state.  The two
 // cells of a thread are processed one after the other (this phase carries the
-// most live values).  Reduction: {closure max, bad max, carbon sum, energy sum}.
+// most live values).  Slots: K, x, phi_a, phi_t, phi_g (stencils), c, chi,
+// icpt.  Reduction: {closure max, bad max, carbon sum, energy sum}.
 __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double& closure, bool& bad,
                             double& mass, double& energy) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const int tr = cur ^ 1;
-    const double* const* tp = B.phi[tr];
-    const double* x = B.x;
-    const double* K = B.K;
     double vclos = 0, vbad = 0, vmass = 0, ven = 0;
-    FOR_TILES(P) {
-        const Pair c = pair_of(P, t);
-        if (!c.v0) continue;
+    const int maps[8] = {kMapK, kMapX, kMapState + 5 * tr, kMapState + 5 * tr + 1, kMapState + 5 * tr + 2,
+                         kMapState + 5 * cur + 3, kMapChi, kMapIcpt};
+    const double* const planes[8] = {B.K, B.x, B.phi[tr][0], B.phi[tr][1], B.phi[tr][2], B.c[cur], B.chi, B.icpt};
+    const bool ok = sweep<8>(a, *red.pipe_ptr, maps, planes, 0x1Fu, [&](const auto& src, const Pair& c) {
 #pragma unroll 1
         for (int k = 0; k < 2; ++k) {
             if (k == 1 && !c.v1) break;
             const int y = c.y0 + k;
             const size_t i = k ? c.i1 : c.i0;
-            const size_t iw = k ? c.iw1 : c.iw0, ie = k ? c.ie1 : c.ie0;
-            const size_t is = k ? c.i0 : c.is0;
-            const size_t in = k ? c.in1 : (c.v1 ? c.i1 : c.i0);
             const bool has_n = y < P.ny - 1;
             Faces f;
-            const double kc = K[i];
-            f.w0 = face_x(P, kc, K[iw]);
-            f.w1 = face_x(P, kc, K[ie]);
-            f.w2 = face_y(P, kc, K[is]);
-            f.w3 = face_y(P, kc, K[in]);
+            const double kc = src.v(0, k, kC);
+            f.w0 = face_x(P, kc, src.v(0, k, kW));
+            f.w1 = face_x(P, kc, src.v(0, k, kE));
+            f.w2 = face_y(P, kc, src.v(0, k, kS));
+            f.w3 = face_y(P, kc, src.v(0, k, kN));
             if (y == 0) f.w2 = 0;
             if (!has_n) f.w3 = 0;
-            const double u = x[i];
-            const double cn = B.c[cur][i] + flux_at(dt, f, u, x[iw], x[ie], x[is], x[in]);
-            const double chi = B.chi[i], icpt = B.icpt[i];
+            const double u = src.v(1, k, kC);
+            const double cn = src.v(5, k, kC) +
+                              flux_at(dt, f, u, src.v(1, k, kW), src.v(1, k, kE), src.v(1, k, kS), src.v(1, k, kN));
+            const double chi = src.v(6, k, kC), icpt = src.v(7, k, kC);
             vclos = fmax(vclos, fabs(cn - (icpt + chi * u)));
             const double mun = P.mu_ref + (cn - icpt) / chi;
             B.c[tr][i] = cn;
             B.mu[tr][i] = mun;
-            const Phi3 q = load_phi(tp, i), e = load_phi(tp, ie);
-            const Phi3 n = has_n ? load_phi(tp, in) : Phi3{0, 0, 0};
+            const Phi3 q{src.v(2, k, kC), src.v(3, k, kC), src.v(4, k, kC)};
+            const Phi3 e{src.v(2, k, kE), src.v(3, k, kE), src.v(4, k, kE)};
+            const Phi3 n = has_n ? Phi3{src.v(2, k, kN), src.v(3, k, kN), src.v(4, k, kN)} : Phi3{0, 0, 0};
             if (bad_cell(P, q, cn, mun)) vbad = 1;
             vmass += cn;
             ven += energy_cell(P, q, e, n, has_n, cn, chi, icpt);
         }
-    }
+    });
+    if (!ok) return false;
     double v[4] = {vclos, vbad, vmass, ven};
     if (!red.reduce<4>(v, OPS4(kMax, kMax, kSum, kSum), kTagFinal)) return false;
     closure = v[0];
@@ -1295,7 +1472,17 @@ __device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
 __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs a) {
     Ctl* ctl = a.B.ctl;
     __shared__ PhaseClock clk;
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    Pipe pipe{reinterpret_cast<uint64_t*>(dsmem), reinterpret_cast<double*>(dsmem + 128), 0u};
+    if (a.use_tma) {
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < kMaxStages; ++s) mbar_init(&pipe.bar[s], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
     Red red(a, &clk);
+    red.pipe_ptr = &pipe;
     StepState st;
     st.S = ctl->S;
     st.cur = ctl->cur;
@@ -1470,6 +1657,8 @@ __global__ void division_selftest_kernel(const double* a, const double* b, const
 using namespace pearl_gpu;
 
 struct pearl_gpu_ctx {
+    CUtensorMap maps[kMapCount];
+    bool use_tma = false;
     int device = 0;
     int nx = 0, ny = 0, pitch = 0;
     cudaStream_t stream = nullptr;
@@ -1489,6 +1678,8 @@ struct pearl_gpu_ctx {
 };
 
 namespace {
+
+constexpr int kDefaultWarpsXLog2 = 0;
 
 const char* why_text(int why) {
     switch (why) {
@@ -1545,8 +1736,17 @@ void fill_dev_params(pearl_gpu_ctx* ctx) {
     P.nx = ctx->nx;
     P.ny = ctx->ny;
     P.pitch = ctx->pitch;
-    P.ntx = (ctx->nx + kTileX - 1) / kTileX;
-    P.nty = (ctx->ny + kTileRows - 1) / kTileRows;
+    // Tile shape: warps side by side in x give longer contiguous row segments
+    // (better DRAM locality); PEARL_GPU_TILE_WARPS_X = 1, 2, 4 or 8 overrides.
+    int wx_log2 = kDefaultWarpsXLog2;
+    if (const char* e = std::getenv("PEARL_GPU_TILE_WARPS_X")) {
+        const int w = std::atoi(e);
+        wx_log2 = w >= 8 ? 3 : w >= 4 ? 2 : w >= 2 ? 1 : 0;
+    }
+    P.warps_x_log2 = wx_log2;
+    const int tile_w = 32 << wx_log2, tile_h = 2 << (3 - wx_log2);
+    P.ntx = (ctx->nx + tile_w - 1) / tile_w;
+    P.nty = (ctx->ny + tile_h - 1) / tile_h;
     P.ntiles = P.ntx * P.nty;
     P.dx = p->dx;
     P.dy = p->dy;
@@ -1630,7 +1830,10 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
     args.B = ctx->B;
     void* kargs[] = {&args};
     PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(ctx->grid), dim3(kThreads), kargs, 0,
+    args.use_tma = ctx->use_tma ? 1 : 0;
+    if (ctx->use_tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(ctx->grid), dim3(kThreads), kargs,
+                                             ctx->use_tma ? kTmaSmemBytes : 0,
                                              ctx->stream));
     ctx->launches++;
     PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
@@ -1665,6 +1868,49 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
 }
 
 size_t plane_elems(const pearl_gpu_ctx* ctx) { return (size_t)ctx->pitch * ctx->ny; }
+
+// 2-D TMA descriptors for the planes the stencil phases stage through shared
+// memory: box (kBoxW x kBoxH) float64, dims (nx, ny), row stride pitch*8 bytes,
+// zero fill outside.  Returns false when the driver cannot encode them; the
+// kernels then read the planes directly.
+bool build_tensor_maps(pearl_gpu_ctx* ctx) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const DevBufs& B = ctx->B;
+    double* planes[kMapCount] = {};
+    for (int s = 0; s < 2; ++s) {
+        for (int a = 0; a < 3; ++a) planes[kMapState + 5 * s + a] = B.phi[s][a];
+        planes[kMapState + 5 * s + 3] = B.c[s];
+        planes[kMapState + 5 * s + 4] = B.mu[s];
+    }
+    planes[kMapK] = B.K;
+    planes[kMapChi] = B.chi;
+    planes[kMapIcpt] = B.icpt;
+    planes[kMapX] = B.x;
+    planes[kMapZ] = B.z;
+    planes[kMapP0] = B.p[0];
+    planes[kMapP1] = B.p[1];
+    planes[kMapWE] = B.wE;
+    planes[kMapWN] = B.wN;
+    for (int m = 0; m < kMapCount; ++m) {
+        const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
+        const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(double)};
+        const cuuint32_t box[2] = {(cuuint32_t)kBoxW, (cuuint32_t)kBoxH};
+        const cuuint32_t estr[2] = {1, 1};
+        if (encode(&ctx->maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, planes[m], dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
 
 // AoS host (ny,nx,3) + two scalar fields <-> padded SoA device planes
 int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* carbon, const double* mu) {
@@ -1776,15 +2022,23 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (!coop) return bail(PEARL_ERR_NO_DEVICE);
+    fill_dev_params(ctx);
+    // TMA staging of the stencil phases needs the 32x16 tile; PEARL_GPU_TMA=0 turns it off.
+    const char* tma_env = std::getenv("PEARL_GPU_TMA");
+    ctx->use_tma = ctx->P.warps_x_log2 == 0 && !(tma_env && std::atoi(tma_env) == 0);
+    if (ctx->use_tma &&
+        cudaFuncSetAttribute(pearl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
+            cudaSuccess)
+        ctx->use_tma = false;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads,
+                                                      ctx->use_tma ? kTmaSmemBytes : 0) != cudaSuccess ||
         per_sm < 1)
         return bail(PEARL_ERR_CUDA);
-    fill_dev_params(ctx);
     ctx->grid = std::max(1, std::min(per_sm * sms, ctx->P.ntiles));
     // state: 2 x (3 phi + c + mu); work: K chi icpt diag x r z p0 p1 Ap  -> 20 planes
     const size_t pe = plane_elems(ctx);
-    const int nplanes = 20;
+    const int nplanes = 22;
     const size_t part = (size_t)2 * ctx->grid * kMaxRed;
     if (cudaMalloc(&ctx->slab, (nplanes * pe + part) * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
     if (cudaMemset(ctx->slab, 0, (nplanes * pe + part) * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
@@ -1806,11 +2060,14 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     ctx->B.p[0] = q; q += pe;
     ctx->B.p[1] = q; q += pe;
     ctx->B.Ap = q; q += pe;
+    ctx->B.wE = q; q += pe;
+    ctx->B.wN = q; q += pe;
     ctx->B.part = q;
     if (cudaMalloc(&ctx->d_ctl, sizeof(Ctl)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
     if (cudaMallocHost(&ctx->h_ctl, sizeof(Ctl)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
     std::memset(ctx->h_ctl, 0, sizeof(Ctl));
     ctx->B.ctl = ctx->d_ctl;
+    if (ctx->use_tma && !build_tensor_maps(ctx)) ctx->use_tma = false;
     ctx->stage_elems = 5 * pe;
     if (cudaMallocHost(&ctx->h_stage, ctx->stage_elems * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
@@ -2133,7 +2390,7 @@ namespace {
 
 constexpr long long kNoAllocMaxCells = 262144;  // 512 x 512 cells
 constexpr int kNoAllocMaxBlocks = 4096;         // bound of the cooperative grid
-constexpr int kNoAllocPlanes = 15;              // trial phi(3) c mu + K chi icpt diag x r z p0 p1 Ap
+constexpr int kNoAllocPlanes = 17;  // trial phi(3) c mu + K chi icpt diag x r z p0 p1 Ap wE wN
 constexpr size_t kNoAllocCtlDoubles = (sizeof(Ctl) + 255) / 256 * 32;
 constexpr size_t kNoAllocDoubles =
     kNoAllocPlanes * (size_t)kNoAllocMaxCells + (size_t)2 * kNoAllocMaxBlocks * kMaxRed + kNoAllocCtlDoubles;
@@ -2144,7 +2401,7 @@ double* g_noalloc_device_ptr[kNoAllocMaxDevices] = {};
 
 }  // namespace
 
-// 15 planes of 262144 doubles + partials + control block: about 31.9 MB per GPU.
+// 17 planes of 262144 doubles + partials + control block: about 36 MB per GPU.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 namespace {
@@ -2205,7 +2462,9 @@ extern "C" int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int
     B.z = q; q += pe;
     B.p[0] = q; q += pe;
     B.p[1] = q; q += pe;
-    B.Ap = q;
+    B.Ap = q; q += pe;
+    B.wE = q; q += pe;
+    B.wN = q;
     B.part = scratch + kNoAllocPlanes * (size_t)kNoAllocMaxCells;
     B.ctl = reinterpret_cast<Ctl*>(B.part + (size_t)2 * kNoAllocMaxBlocks * kMaxRed);
 
