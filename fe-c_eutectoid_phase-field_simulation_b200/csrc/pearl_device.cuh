@@ -194,9 +194,9 @@ constexpr int kBoxW = kTileX + 4;
 constexpr int kBoxH = kTileRows + 2;
 constexpr uint32_t kBoxBytes = kBoxW * kBoxH * sizeof(double);        // 5184
 constexpr int kFieldStride = ((kBoxBytes + 127) / 128 * 128) / 8;     // doubles per staged field (128 B aligned)
-constexpr int kMaxStageFields = 8;
+constexpr int kMaxStageFields = 9;
 constexpr int kMaxStages = 4;
-// Shared-memory budget of the pipeline: two stages of the widest phase (8 fields);
+// Shared-memory budget of the pipeline: two stages of the widest phase (9 fields);
 // phases staging fewer fields run more stages in the same space (up to 4).
 constexpr size_t kPipeDoubles = (size_t)2 * kMaxStageFields * kFieldStride;
 constexpr size_t kTmaSmemBytes = 128 + kPipeDoubles * sizeof(double);

@@ -473,8 +473,11 @@ __device__ __forceinline__ Proposal propose_cell(const DevParams& P, const Src& 
     for (int aa = 0; aa < 3; ++aa) {
         const double qa1 = q[(aa + 1) % 3], qa2 = q[(aa + 2) % 3];
         f[aa] = P.obs * (qa1 + qa2) + P.tr * qa1 * qa2;
+        // b = gamma contributes (psi_g - psi_g)*dh/Vm = +-0, which leaves every
+        // finite force unchanged (a non-finite dh makes the other terms
+        // non-finite too), so only alpha and theta are added.
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
+        for (int b = 0; b < 2; ++b) {
             const double dh = dtr[aa] + (b == aa ? 6.0 * q[b] * (1.0 - q[b]) : 0.0);
             f[aa] += div_by(P, (ps[b] - psi0) * dh, P.Vm, P.r_Vm);
         }
@@ -789,43 +792,37 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
 // FINAL: carbon update, closure and mu (pearl_serial.cpp:1082-1093) fused with
 // valid_state, total_carbon and reduced_energy of the trial state.  The two
 // cells of a thread are processed one after the other (this phase carries the
-// most live values).  Slots: K, x, phi_a, phi_t, phi_g (stencils), c, chi,
-// icpt.  Reduction: {closure max, bad max, carbon sum, energy sum}.
+// most live values).  Slots: wE, wN, x, phi_a, phi_t, phi_g (stencils), c,
+// chi, icpt.  Reduction: {closure max, bad max, carbon sum, energy sum}.
 __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double& closure, bool& bad,
                             double& mass, double& energy) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const int tr = cur ^ 1;
     double vclos = 0, vbad = 0, vmass = 0, ven = 0;
-    const int maps[8] = {kMapK, kMapX, kMapState + 5 * tr, kMapState + 5 * tr + 1, kMapState + 5 * tr + 2,
+    const int maps[9] = {kMapWE, kMapWN, kMapX, kMapState + 5 * tr, kMapState + 5 * tr + 1, kMapState + 5 * tr + 2,
                          kMapState + 5 * cur + 3, kMapChi, kMapIcpt};
-    const double* const planes[8] = {B.K, B.x, B.phi[tr][0], B.phi[tr][1], B.phi[tr][2], B.c[cur], B.chi, B.icpt};
-    const bool ok = sweep<8>(a, *red.pipe_ptr, maps, planes, 0x1Fu, [&](const auto& src, const Pair& c) {
+    const double* const planes[9] = {B.wE, B.wN, B.x, B.phi[tr][0], B.phi[tr][1], B.phi[tr][2], B.c[cur], B.chi,
+                                     B.icpt};
+    const bool ok = sweep<9>(a, *red.pipe_ptr, maps, planes, 0x3Fu, [&](const auto& src, const Pair& c) {
 #pragma unroll 1
         for (int k = 0; k < 2; ++k) {
             if (k == 1 && !c.v1) break;
             const int y = c.y0 + k;
             const size_t i = k ? c.i1 : c.i0;
             const bool has_n = y < P.ny - 1;
-            Faces f;
-            const double kc = src.v(0, k, kC);
-            f.w0 = face_x(P, kc, src.v(0, k, kW));
-            f.w1 = face_x(P, kc, src.v(0, k, kE));
-            f.w2 = face_y(P, kc, src.v(0, k, kS));
-            f.w3 = face_y(P, kc, src.v(0, k, kN));
-            if (y == 0) f.w2 = 0;
-            if (!has_n) f.w3 = 0;
-            const double u = src.v(1, k, kC);
-            const double cn = src.v(5, k, kC) +
-                              flux_at(dt, f, u, src.v(1, k, kW), src.v(1, k, kE), src.v(1, k, kS), src.v(1, k, kN));
-            const double chi = src.v(6, k, kC), icpt = src.v(7, k, kC);
+            const Faces f = faces_stored(src, 0, 1, k, c);
+            const double u = src.v(2, k, kC);
+            const double cn = src.v(6, k, kC) +
+                              flux_at(dt, f, u, src.v(2, k, kW), src.v(2, k, kE), src.v(2, k, kS), src.v(2, k, kN));
+            const double chi = src.v(7, k, kC), icpt = src.v(8, k, kC);
             vclos = fmax(vclos, fabs(cn - (icpt + chi * u)));
             const double mun = P.mu_ref + (cn - icpt) / chi;
             B.c[tr][i] = cn;
             B.mu[tr][i] = mun;
-            const Phi3 q{src.v(2, k, kC), src.v(3, k, kC), src.v(4, k, kC)};
-            const Phi3 e{src.v(2, k, kE), src.v(3, k, kE), src.v(4, k, kE)};
-            const Phi3 n = has_n ? Phi3{src.v(2, k, kN), src.v(3, k, kN), src.v(4, k, kN)} : Phi3{0, 0, 0};
+            const Phi3 q{src.v(3, k, kC), src.v(4, k, kC), src.v(5, k, kC)};
+            const Phi3 e{src.v(3, k, kE), src.v(4, k, kE), src.v(5, k, kE)};
+            const Phi3 n = has_n ? Phi3{src.v(3, k, kN), src.v(4, k, kN), src.v(5, k, kN)} : Phi3{0, 0, 0};
             if (bad_cell(P, q, cn, mun)) vbad = 1;
             vmass += cn;
             ven += energy_cell(P, q, e, n, has_n, cn, chi, icpt);
