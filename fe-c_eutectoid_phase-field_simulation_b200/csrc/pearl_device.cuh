@@ -205,7 +205,8 @@ constexpr size_t kTmaSmemBytes = 128 + kPipeDoubles * sizeof(double);
 // 5*s + f, then the work planes.
 enum MapId : int {
     kMapState = 0,  // + 5*set + field
-    kMapK = 10, kMapChi, kMapIcpt, kMapX, kMapZ, kMapP0, kMapP1, kMapWE, kMapWN, kMapCount
+    kMapK = 10, kMapChi, kMapIcpt, kMapX, kMapZ, kMapP0, kMapP1, kMapWE, kMapWN, kMapR, kMapAp, kMapDiag,
+    kMapCount
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -697,25 +697,16 @@ __device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, dou
 }
 
 // UPDATE: x += alpha p; r -= alpha Ap; z = r/diag; {<r,z>, <r,r>}.
+// Slots (no stencils): x, p, r, Ap, diag.
 __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
-    const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    const double* p = B.p[pcur];
     double s0 = 0, s1 = 0;
-    FOR_TILES(P) {
-        const Pair c = pair_of(P, t);
-        if (!c.v0) continue;
-        const double x0 = B.x[c.i0], p0 = p[c.i0], r0 = B.r[c.i0], A0 = B.Ap[c.i0], d0 = B.diag[c.i0];
-        double x1 = 0, p1 = 0, r1 = 0, A1 = 0, d1 = 1;
-        if (c.v1) {
-            x1 = B.x[c.i1];
-            p1 = p[c.i1];
-            r1 = B.r[c.i1];
-            A1 = B.Ap[c.i1];
-            d1 = B.diag[c.i1];
-        }
+    const int maps[5] = {kMapX, pcur ? kMapP1 : kMapP0, kMapR, kMapAp, kMapDiag};
+    const double* const planes[5] = {B.x, B.p[pcur], B.r, B.Ap, B.diag};
+    const bool ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x0u, [&](const auto& src, const Pair& c) {
         {
-            const double x = x0 + alpha * p0, r = r0 - alpha * A0, z = r / d0;
+            const double x = src.v(0, 0, kC) + alpha * src.v(1, 0, kC), r = src.v(2, 0, kC) - alpha * src.v(3, 0, kC);
+            const double z = r / src.v(4, 0, kC);
             B.x[c.i0] = x;
             B.r[c.i0] = r;
             B.z[c.i0] = z;
@@ -723,14 +714,16 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
             s1 += r * r;
         }
         if (c.v1) {
-            const double x = x1 + alpha * p1, r = r1 - alpha * A1, z = r / d1;
+            const double x = src.v(0, 1, kC) + alpha * src.v(1, 1, kC), r = src.v(2, 1, kC) - alpha * src.v(3, 1, kC);
+            const double z = r / src.v(4, 1, kC);
             B.x[c.i1] = x;
             B.r[c.i1] = r;
             B.z[c.i1] = z;
             s0 += r * z;
             s1 += r * r;
         }
-    }
+    });
+    if (!ok) return false;
     double v[2] = {s0, s1};
     if (!red.reduce<2>(v, OPS2(kSum, kSum), kTagUpdate)) return false;
     rz = v[0];
@@ -1896,6 +1889,9 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
     planes[kMapP1] = B.p[1];
     planes[kMapWE] = B.wE;
     planes[kMapWN] = B.wN;
+    planes[kMapR] = B.r;
+    planes[kMapAp] = B.Ap;
+    planes[kMapDiag] = B.diag;
     for (int m = 0; m < kMapCount; ++m) {
         const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
         const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(double)};
