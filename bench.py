@@ -32,7 +32,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import time
 from pathlib import Path
@@ -108,51 +107,69 @@ def ncu_traffic_per_cell():
 
 
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled during the timed region.
 
-    def __init__(self, index: int):
+    Uses NVML from a background thread every few milliseconds (read-only
+    queries), so even a short timed region yields many samples; falls back to
+    `nvidia-smi -lms` when NVML is unavailable."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, index: int, period_s: float = 0.005):
         self.index = index
-        self.proc = None
-        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"pearl_clocks_{os.getpid()}.csv"
+        self.period = period_s
+        self.samples: list[tuple[float, float, int]] = []
+        self._stop = None
+        self._thread = None
+        self._nvml = None
 
     def start(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        except Exception:  # noqa: BLE001 - no NVML: nothing sampled
+            self._nvml = None
+            return
+        self._stop = threading.Event()
+
+        def run():
+            P = self._nvml
+            get_reasons = getattr(P, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                P.nvmlDeviceGetCurrentClocksThrottleReasons
+            max_mhz = float(P.nvmlDeviceGetMaxClockInfo(handle, P.NVML_CLOCK_SM))
+            while not self._stop.is_set():
+                try:
+                    sm = float(P.nvmlDeviceGetClockInfo(handle, P.NVML_CLOCK_SM))
+                    reasons = int(get_reasons(handle))
+                except Exception:  # noqa: BLE001
+                    break
+                self.samples.append((sm, max_mhz, reasons))
+                self._stop.wait(self.period)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
 
     def stop(self) -> dict | None:
-        if self.proc is None:
+        if self._thread is None:
             return None
-        self.proc.terminate()
+        self._stop.set()
+        self._thread.join(timeout=5)
         try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = []
-        for line in self.path.read_text().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                rows.append((float(f[1]), float(f[2]), f[5:9]))
-            except ValueError:
-                continue
-        try:
-            self.path.unlink()
-        except OSError:
+            self._nvml.nvmlShutdown()
+        except Exception:  # noqa: BLE001
             pass
-        if not rows:
+        if not self.samples:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower().startswith("active")})
-        sm = [s for s, _, _ in rows]
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(m for _, m, _ in rows), "reasons": reasons,
-                "samples": len(rows)}
+        reasons = sorted(name for name, bit in self.REASONS.items() if any(r & bit for _, _, r in self.samples))
+        sm = [s for s, _, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(m for _, m, _ in self.samples),
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml"}
 
 
 def reduce_over_ranks(dist, x: float, op: str, device: str) -> float:

@@ -9,10 +9,10 @@
 //   SETUP    implicit_diffusion set-up: apply(mu_offset), r, z, diag (:1021-1046)
 //   APPLY    p = z + beta p ; A p ; <p,Ap>                          (:1067-1079)
 //   UPDATE   x += alpha p ; r -= alpha Ap ; z = r/diag ; <r,z>,<r,r> (:1071-1078)
-//   TRUE_RES r = rhs - A x ; <r,r>                                   (:1051-1055)
-//   RESET    z = r/diag ; <r,z>                                      (:1060-1064)
-//   FINAL    conservative carbon update, closure, mu, valid_state,
-//            total_carbon and reduced_energy of the trial state      (:1082-1093, :1096-1116, :784-821)
+//   FINAL    true residual r = rhs - A x (:1051-1055) fused with the conservative
+//            carbon update, closure, mu, valid_state, total_carbon and
+//            reduced_energy of the trial state (:1082-1093, :1096-1116, :784-821)
+//   RESET    z = r/diag ; <r,z> when the true residual misses     (:1060-1064)
 //
 // Thread mapping: a warp covers 32 consecutive x of two adjacent rows; the
 // eight warps of a block stack 16 rows.  The two cells of a thread share their
@@ -731,35 +731,6 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
     return true;
 }
 
-// TRUE_RES: r = rhs - A x; <r,r>  (pearl_serial.cpp:1051-1055)
-// Slots: wE, wN, x (stencils), chi, icpt, c.
-__device__ bool phase_true_residual(const KArgs& a, Red& red, int cur, double dt, double& rr) {
-    const DevBufs& B = a.B;
-    double s = 0;
-    const int maps[6] = {kMapWE, kMapWN, kMapX, kMapChi, kMapIcpt, kMapState + 5 * cur + 3};
-    const double* const planes[6] = {B.wE, B.wN, B.x, B.chi, B.icpt, B.c[cur]};
-    const bool ok = sweep<6>(a, *red.pipe_ptr, maps, planes, 0x7u, [&](const auto& src, const Pair& c) {
-        const S2 x = stencil2(src, 2, c.v1);
-        {
-            const double r = (src.v(5, 0, kC) - src.v(4, 0, kC)) -
-                             apply0(src.v(3, 0, kC), dt, faces_stored(src, 0, 1, 0, c), x);
-            B.r[c.i0] = r;
-            s += r * r;
-        }
-        if (c.v1) {
-            const double r = (src.v(5, 1, kC) - src.v(4, 1, kC)) -
-                             apply1(src.v(3, 1, kC), dt, faces_stored(src, 0, 1, 1, c), x);
-            B.r[c.i1] = r;
-            s += r * r;
-        }
-    });
-    if (!ok) return false;
-    double v[1] = {s};
-    if (!red.reduce<1>(v, kSum, kTagTrueRes)) return false;
-    rr = v[0];
-    return true;
-}
-
 // RESET: z = r/diag; <r,z>  (pearl_serial.cpp:1060-1064)
 __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
     const DevParams& P = a.P;
@@ -782,17 +753,20 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
     return true;
 }
 
-// FINAL: carbon update, closure and mu (pearl_serial.cpp:1082-1093) fused with
-// valid_state, total_carbon and reduced_energy of the trial state.  The two
-// cells of a thread are processed one after the other (this phase carries the
-// most live values).  Slots: wE, wN, x, phi_a, phi_t, phi_g (stencils), c,
-// chi, icpt.  Reduction: {closure max, bad max, carbon sum, energy sum}.
+// FINAL: the true residual check of the converged solve (pearl_serial.cpp:1051-1055)
+// fused with the carbon update, closure and mu (:1082-1093), valid_state,
+// total_carbon and reduced_energy of the trial state.  Everything after the
+// residual is speculative: the caller uses it only when the residual passes,
+// and otherwise restarts CG from the r written here.  The two cells of a
+// thread are processed one after the other (this phase carries the most live
+// values).  Slots: wE, wN, x, phi_a, phi_t, phi_g (stencils), c, chi, icpt.
+// Reduction: {closure max, bad max, carbon sum, energy sum, <r,r>}.
 __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double& closure, bool& bad,
-                            double& mass, double& energy) {
+                            double& mass, double& energy, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const int tr = cur ^ 1;
-    double vclos = 0, vbad = 0, vmass = 0, ven = 0;
+    double vclos = 0, vbad = 0, vmass = 0, ven = 0, vrr = 0;
     const int maps[9] = {kMapWE, kMapWN, kMapX, kMapState + 5 * tr, kMapState + 5 * tr + 1, kMapState + 5 * tr + 2,
                          kMapState + 5 * cur + 3, kMapChi, kMapIcpt};
     const double* const planes[9] = {B.wE, B.wN, B.x, B.phi[tr][0], B.phi[tr][1], B.phi[tr][2], B.c[cur], B.chi,
@@ -806,9 +780,13 @@ __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double
             const bool has_n = y < P.ny - 1;
             const Faces f = faces_stored(src, 0, 1, k, c);
             const double u = src.v(2, k, kC);
-            const double cn = src.v(6, k, kC) +
-                              flux_at(dt, f, u, src.v(2, k, kW), src.v(2, k, kE), src.v(2, k, kS), src.v(2, k, kN));
+            const double uw = src.v(2, k, kW), ue = src.v(2, k, kE), us = src.v(2, k, kS), un = src.v(2, k, kN);
+            const double cold = src.v(6, k, kC);
             const double chi = src.v(7, k, kC), icpt = src.v(8, k, kC);
+            const double r = (cold - icpt) - apply_at(chi, dt, f, u, uw, ue, us, un);
+            B.r[i] = r;
+            vrr += r * r;
+            const double cn = cold + flux_at(dt, f, u, uw, ue, us, un);
             vclos = fmax(vclos, fabs(cn - (icpt + chi * u)));
             const double mun = P.mu_ref + (cn - icpt) / chi;
             B.c[tr][i] = cn;
@@ -822,12 +800,13 @@ __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double
         }
     });
     if (!ok) return false;
-    double v[4] = {vclos, vbad, vmass, ven};
-    if (!red.reduce<4>(v, OPS4(kMax, kMax, kSum, kSum), kTagFinal)) return false;
+    double v[5] = {vclos, vbad, vmass, ven, vrr};
+    if (!red.reduce<5>(v, OPS5(kMax, kMax, kSum, kSum, kSum), kTagFinal)) return false;
     closure = v[0];
     bad = v[1] != 0;
     mass = v[2] * P.dx * P.dy;
     energy = v[3] * P.dx * P.dy;
+    rr = v[4];
     return true;
 }
 
@@ -931,12 +910,17 @@ __device__ bool diffusion(const KArgs& a, Red& red, int cur, double dt, Diffusio
         o.residual = sqrt(rr);
         if (!isfinite(o.residual)) return true;
         if (o.residual <= tolerance) {
-            if (!phase_true_residual(a, red, cur, dt, rr)) return false;
+            // true residual (pearl_serial.cpp:1051-1055) in the same pass as the final update
+            if (!phase_final(a, red, cur, dt, o.closure, o.bad, o.mass, o.energy, rr)) return false;
             o.residual = sqrt(rr);
             if (o.residual <= tolerance * 1.05) {
                 o.ok = true;
                 break;
             }
+            o.closure = 0;
+            o.bad = false;
+            o.mass = 0;
+            o.energy = 0;
             if (!phase_reset(a, red, rz)) return false;
             first = true;
             continue;
@@ -955,7 +939,6 @@ __device__ bool diffusion(const KArgs& a, Red& red, int cur, double dt, Diffusio
         first = false;
     }
     if (!o.ok) return true;
-    if (!phase_final(a, red, cur, dt, o.closure, o.bad, o.mass, o.energy)) return false;
     o.ok = o.closure <= P.closure_tol;
     return true;
 }
