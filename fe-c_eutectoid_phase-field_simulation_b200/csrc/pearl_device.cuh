@@ -299,7 +299,7 @@ __device__ __forceinline__ double red_identity(unsigned op) {
 __device__ __forceinline__ unsigned op_of(unsigned ops, int k) { return (ops >> (2 * k)) & 3u; }
 
 template <int NV>
-__device__ __forceinline__ void block_publish(const double (&v)[NV], unsigned ops, double* part_slot) {
+__device__ __forceinline__ void block_publish(const double (&v)[NV], unsigned ops, double* part_slot, int bid) {
     __shared__ double s_red[kThreads / 32][kMaxRed];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -317,13 +317,13 @@ __device__ __forceinline__ void block_publish(const double (&v)[NV], unsigned op
             const unsigned op = op_of(ops, k);
             double acc = s_red[0][k];
             for (int w = 1; w < kThreads / 32; ++w) acc = red_apply(op, acc, s_red[w][k]);
-            part_slot[blockIdx.x * kMaxRed + k] = acc;
+            part_slot[bid * kMaxRed + k] = acc;
         }
     }
 }
 
 template <int NV>
-__device__ __forceinline__ void grid_gather(double (&out)[NV], unsigned ops, const double* part_slot) {
+__device__ __forceinline__ void grid_gather(double (&out)[NV], unsigned ops, const double* part_slot, int nblk) {
     __shared__ double s_out[kMaxRed];
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
@@ -331,7 +331,7 @@ __device__ __forceinline__ void grid_gather(double (&out)[NV], unsigned ops, con
         for (int k = 0; k < NV; ++k) {
             const unsigned op = op_of(ops, k);
             double acc = red_identity(op);
-            for (int b = lane; b < (int)gridDim.x; b += 32) acc = red_apply(op, acc, part_slot[b * kMaxRed + k]);
+            for (int b = lane; b < nblk; b += 32) acc = red_apply(op, acc, part_slot[b * kMaxRed + k]);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc = red_apply(op, acc, __shfl_down_sync(0xffffffffu, acc, o));
             if (lane == 0) s_out[k] = acc;

@@ -64,6 +64,24 @@ struct KArgs {
     double init_mu;
 };
 
+// One domain as seen by one block: its parameters, buffers and tensor maps,
+// the block's index in the group of blocks that shares the domain, the
+// group's barrier words and error status, and its reduction partials.  A
+// single-domain launch is one group spanning the whole grid; a batched launch
+// gives every group of blocks its own instances.
+struct Dom {
+    const DevParams& P;
+    const DevBufs& B;
+    const CUtensorMap* maps;
+    int use_tma;
+    int bid, nblk;
+    Ctl* bar;      // barrier words and status of this block group
+    double* part;  // [2][nblk][kMaxRed] partials of this block group
+    double shift_trigger, shift_target, shift_c_gamma;
+    int smooth_max_steps, smooth_min_steps;
+    double smooth_energy_rtol, smooth_max_phase_change;
+};
+
 // The two cells (x, y0) and (x, y0+1) of one thread in tile t.
 struct Pair {
     int x, y0;
@@ -242,12 +260,12 @@ struct PhaseClock {
 };
 
 struct Red {
-    const KArgs& a;
+    const Dom& a;
     PhaseClock* clk;  // shared memory; used by thread 0 of block 0 only
     unsigned counter = 0;
     struct Pipe* pipe_ptr = nullptr;
-    __device__ Red(const KArgs& args, PhaseClock* c) : a(args), clk(c) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+    __device__ Red(const Dom& args, PhaseClock* c) : a(args), clk(c) {
+        if (a.bid == 0 && threadIdx.x == 0) {
             clk->t_last = globaltimer_ns();
             for (int k = 0; k < kTagCount; ++k) {
                 clk->ns[k] = 0;
@@ -260,21 +278,21 @@ struct Red {
     __device__ bool reduce(double (&v)[NV], unsigned ops, int tag) {
         // this thread's plane stores may be read by TMA (async proxy) after the barrier
         if (a.use_tma) fence_proxy_async();
-        double* slot = a.B.part + (size_t)(counter & 1u) * gridDim.x * kMaxRed;
+        double* slot = a.part + (size_t)(counter & 1u) * a.nblk * kMaxRed;
         ++counter;
-        block_publish<NV>(v, ops, slot);
-        if (!grid_barrier(a.B.ctl, gridDim.x)) return false;
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        block_publish<NV>(v, ops, slot, a.bid);
+        if (!grid_barrier(a.bar, a.nblk)) return false;
+        if (a.bid == 0 && threadIdx.x == 0) {
             const unsigned long long t = globaltimer_ns();
             clk->ns[tag] += t - clk->t_last;
             clk->cnt[tag] += 1;
             clk->t_last = t;
         }
-        grid_gather<NV>(v, ops, slot);
+        grid_gather<NV>(v, ops, slot, a.nblk);
         return true;
     }
     __device__ void flush() const {
-        if (blockIdx.x == 0 && threadIdx.x == 0)
+        if (a.bid == 0 && threadIdx.x == 0)
             for (int k = 0; k < kTagCount; ++k) {
                 a.B.ctl->phase_ns[k] = clk->ns[k];
                 a.B.ctl->phase_count[k] = clk->cnt[k];
@@ -287,7 +305,7 @@ struct Red {
 #define OPS4(a, b, c, d) (OPS3(a, b, c) | ((unsigned)(d) << 6))
 #define OPS5(a, b, c, d, e) (OPS4(a, b, c, d) | ((unsigned)(e) << 8))
 
-#define FOR_TILES(P) for (int t = blockIdx.x; t < (P).ntiles; t += gridDim.x)
+#define FOR_TILES(P) for (int t = a.bid; t < (P).ntiles; t += a.nblk)
 
 // ------------------------------------------------------------------ stencil sources
 // A phase body reads its input fields through a source that maps a field slot
@@ -381,7 +399,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // periodic x wrap patched from `planes`.  Returns false after a bounded wait
 // ran out (the status is recorded; in-flight copies are drained, bounded).
 template <int NF, class Body>
-__device__ bool sweep(const KArgs& a, Pipe& pp, const int (&maps)[NF], const double* const (&planes)[NF],
+__device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const double* const (&planes)[NF],
                       unsigned stencil, Body&& body) {
     const DevParams& P = a.P;
     if (!a.use_tma) {
@@ -400,11 +418,11 @@ __device__ bool sweep(const KArgs& a, Pipe& pp, const int (&maps)[NF], const dou
                           ? (int)(kPipeDoubles / ((size_t)NF * kFieldStride))
                           : kMaxStages;
     static_assert(S >= 2, "pipeline needs two stages");
-    const int G = gridDim.x;
-    const int nb = (int)blockIdx.x < P.ntiles ? (P.ntiles - 1 - (int)blockIdx.x) / G + 1 : 0;
+    const int G = a.nblk;
+    const int nb = a.bid < P.ntiles ? (P.ntiles - 1 - a.bid) / G + 1 : 0;
     const auto issue = [&](int k) {
         if (threadIdx.x != 0) return;
-        const int t = blockIdx.x + k * G;
+        const int t = a.bid + k * G;
         const int bx = t % P.ntx, by = t / P.ntx;
         const int s = k % S;
         double* dst = pp.stage + (size_t)s * NF * kFieldStride;
@@ -420,13 +438,13 @@ __device__ bool sweep(const KArgs& a, Pipe& pp, const int (&maps)[NF], const dou
         const int s = k % S;
         if (k + S - 1 < nb) issue(k + S - 1);
         if (!mbar_wait_bounded(&pp.bar[s], (pp.parity >> s) & 1u)) {
-            atomicCAS(&a.B.ctl->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
+            atomicCAS(&a.bar->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
             for (int j = k + 1; j < nb && j < k + S; ++j)  // drain the copies still in flight, bounded
                 mbar_wait_bounded(&pp.bar[j % S], (pp.parity >> (j % S)) & 1u);
             return false;
         }
         pp.parity ^= 1u << s;
-        const int t = blockIdx.x + k * G;
+        const int t = a.bid + k * G;
         const int bx = t % P.ntx, by = t / P.ntx;
         double* st = pp.stage + (size_t)s * NF * kFieldStride;
         const bool left = bx == 0, right = (bx + 1) * kTileX >= P.nx;
@@ -521,7 +539,7 @@ __device__ __forceinline__ Proposal propose_cell(const DevParams& P, const Src& 
 // the trial phi (K, chi, icpt); in phase_only mode also the reconstructed
 // trial carbon and the copied trial mu (pearl_serial.cpp:1134-1136).
 // Reduction: {max |dphi| (inf if non-finite), mixture invalid, simplex failed}.
-__device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, double& change, bool& mixbad,
+__device__ bool phase_propose(const Dom& a, Red& red, int cur, double dt, double& change, bool& mixbad,
                               bool& simplexbad) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
@@ -567,7 +585,7 @@ __device__ bool phase_propose(const KArgs& a, Red& red, int cur, double dt, doub
 }
 
 // MIX: K, chi, icpt of the trial phi (used when the trial phi was uploaded).
-__device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
+__device__ bool phase_mix(const Dom& a, Red& red, int cur, bool& mixbad) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double* const* tp = B.phi[cur ^ 1];
@@ -592,7 +610,7 @@ __device__ bool phase_mix(const KArgs& a, Red& red, int cur, bool& mixbad) {
 
 // SETUP: apply(mu_offset) and the initial residual (pearl_serial.cpp:1036-1046).
 // Slots: K, mu (stencils), chi, icpt, c.  Reduction: {<rhs,rhs>, <r,z>, <r,r>}.
-__device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double& rhs2, double& rz, double& rr) {
+__device__ bool phase_setup(const Dom& a, Red& red, int cur, double dt, double& rhs2, double& rz, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double s0 = 0, s1 = 0, s2 = 0;
@@ -651,7 +669,7 @@ __device__ bool phase_setup(const KArgs& a, Red& red, int cur, double dt, double
 
 // APPLY: p_new = z (first) or z + beta*p_old, written to p[pout]; Ap; <p,Ap>.
 // Slots: wE, wN, z (stencils), chi, p_old (stencil).
-__device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
+__device__ bool phase_apply(const Dom& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
     const DevBufs& B = a.B;
     double* pn = B.p[pout];
     double s = 0;
@@ -698,7 +716,7 @@ __device__ bool phase_apply(const KArgs& a, Red& red, double dt, bool first, dou
 
 // UPDATE: x += alpha p; r -= alpha Ap; z = r/diag; {<r,z>, <r,r>}.
 // Slots (no stencils): x, p, r, Ap, diag.
-__device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
+__device__ bool phase_update(const Dom& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
     const DevBufs& B = a.B;
     double s0 = 0, s1 = 0;
     const int maps[5] = {kMapX, pcur ? kMapP1 : kMapP0, kMapR, kMapAp, kMapDiag};
@@ -732,7 +750,7 @@ __device__ bool phase_update(const KArgs& a, Red& red, double alpha, int pcur, d
 }
 
 // RESET: z = r/diag; <r,z>  (pearl_serial.cpp:1060-1064)
-__device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
+__device__ bool phase_reset(const Dom& a, Red& red, double& rz) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     double s = 0;
@@ -761,7 +779,7 @@ __device__ bool phase_reset(const KArgs& a, Red& red, double& rz) {
 // thread are processed one after the other (this phase carries the most live
 // values).  Slots: wE, wN, x, phi_a, phi_t, phi_g (stencils), c, chi, icpt.
 // Reduction: {closure max, bad max, carbon sum, energy sum, <r,r>}.
-__device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double& closure, bool& bad,
+__device__ bool phase_final(const Dom& a, Red& red, int cur, double dt, double& closure, bool& bad,
                             double& mass, double& energy, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
@@ -814,7 +832,7 @@ __device__ bool phase_final(const KArgs& a, Red& red, int cur, double dt, double
 // (ENERGY) or taken from the trial mixture buffers (phase-only FINAL).
 // Accumulates in the same order as phase_final, so equal states give equal sums.
 template <bool kFromBuffers>
-__device__ void energy_sweep(const KArgs& a, int s, double& ven, double& vmass, double& vmix, double& vbad) {
+__device__ void energy_sweep(const Dom& a, int s, double& ven, double& vmass, double& vmix, double& vbad) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const double* const* ph = B.phi[s];
@@ -849,7 +867,7 @@ __device__ void energy_sweep(const KArgs& a, int s, double& ven, double& vmass, 
 
 // PHASE_ONLY FINAL: valid_state and reduced_energy of the trial state whose
 // carbon and mu were written by PROPOSE.  Reduction: {bad max, energy sum}.
-__device__ bool phase_final_phase_only(const KArgs& a, Red& red, int cur, bool& bad, double& energy) {
+__device__ bool phase_final_phase_only(const Dom& a, Red& red, int cur, bool& bad, double& energy) {
     double ven = 0, vmass = 0, vmix = 0, vbad = 0;
     energy_sweep<true>(a, cur ^ 1, ven, vmass, vmix, vbad);
     double v[2] = {vbad, ven};
@@ -862,7 +880,7 @@ __device__ bool phase_final_phase_only(const KArgs& a, Red& red, int cur, bool& 
 // ENERGY: reduced_energy and total_carbon of state `s` (the e0, mass0 of
 // advance, pearl_serial.cpp:1122-1123), plus mixture validity and
 // valid_state.  Reduction: {energy sum, carbon sum, mixture invalid, bad}.
-__device__ bool phase_energy(const KArgs& a, Red& red, int s, double& energy, double& mass, bool& mixbad,
+__device__ bool phase_energy(const Dom& a, Red& red, int s, double& energy, double& mass, bool& mixbad,
                              bool& bad) {
     double ven = 0, vmass = 0, vmix = 0, vbad = 0;
     energy_sweep<false>(a, s, ven, vmass, vmix, vbad);
@@ -875,9 +893,9 @@ __device__ bool phase_energy(const KArgs& a, Red& red, int s, double& energy, do
     return true;
 }
 
-__device__ __forceinline__ void set_error(Ctl* ctl, int status, int why) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (atomicCAS(&ctl->status, 0, status) == 0) ctl->why = why;
+__device__ __forceinline__ void set_error(const Dom& a, int status, int why) {
+    if (a.bid == 0 && threadIdx.x == 0) {
+        if (atomicCAS(&a.bar->status, 0, status) == 0) a.bar->why = why;
     }
 }
 
@@ -890,7 +908,7 @@ struct DiffusionOut {
     bool bad;
 };
 
-__device__ bool diffusion(const KArgs& a, Red& red, int cur, double dt, DiffusionOut& o) {
+__device__ bool diffusion(const Dom& a, Red& red, int cur, double dt, DiffusionOut& o) {
     const DevParams& P = a.P;
     o.ok = false;
     o.it = 0;
@@ -953,14 +971,14 @@ struct StepState {
     double e0, mass0;
 };
 
-__device__ bool advance(const KArgs& a, Red& red, StepState& st, double stop_time, pearl_step_info& info) {
+__device__ bool advance(const Dom& a, Red& red, StepState& st, double stop_time, pearl_step_info& info) {
     const DevParams& P = a.P;
     Ctl* ctl = a.B.ctl;
     double dt = st.S.dt;
     if (P.dt_max < dt) dt = P.dt_max;
     if (stop_time - st.S.time < dt) dt = stop_time - st.S.time;
     if (!(dt > 0) || !isfinite(dt)) {
-        set_error(ctl, PEARL_ERR_INVALID_ADVANCE_TIME, 0);
+        set_error(a, PEARL_ERR_INVALID_ADVANCE_TIME, 0);
         return false;
     }
     if (!st.cache_valid) {
@@ -968,7 +986,7 @@ __device__ bool advance(const KArgs& a, Red& red, StepState& st, double stop_tim
         bool mixbad, bad;
         if (!phase_energy(a, red, st.cur, e, m, mixbad, bad)) return false;
         if (mixbad) {
-            set_error(ctl, PEARL_ERR_MIXTURE, 0);
+            set_error(a, PEARL_ERR_MIXTURE, 0);
             return false;
         }
         st.e0 = P.check_energy ? e : 0;
@@ -984,7 +1002,7 @@ __device__ bool advance(const KArgs& a, Red& red, StepState& st, double stop_tim
         bool mixbad, simplexbad;
         if (!phase_propose(a, red, st.cur, dt, out.max_phase_change, mixbad, simplexbad)) return false;
         if (simplexbad) {
-            set_error(ctl, PEARL_ERR_SIMPLEX, 0);
+            set_error(a, PEARL_ERR_SIMPLEX, 0);
             return false;
         }
         bool good = isfinite(out.max_phase_change) && out.max_phase_change <= P.max_phase_change;
@@ -993,7 +1011,7 @@ __device__ bool advance(const KArgs& a, Red& red, StepState& st, double stop_tim
         double mass = 0, e1 = 0;
         if (good) {
             if (mixbad) {
-                set_error(ctl, PEARL_ERR_MIXTURE, 0);
+                set_error(a, PEARL_ERR_MIXTURE, 0);
                 return false;
             }
             if (P.phase_only) {
@@ -1039,16 +1057,16 @@ __device__ bool advance(const KArgs& a, Red& red, StepState& st, double stop_tim
         }
         dt *= .5;
         if (dt < P.dt_min) {
-            set_error(ctl, PEARL_ERR_REJECTED_BELOW_DT_MIN, why);
+            set_error(a, PEARL_ERR_REJECTED_BELOW_DT_MIN, why);
             return false;
         }
     }
-    set_error(ctl, PEARL_ERR_RETRY_LIMIT, why);
+    set_error(a, PEARL_ERR_RETRY_LIMIT, why);
     return false;
 }
 
 // Moving window on the device (maybe_shift + shift_rows, pearl_serial.cpp:2023-2071).
-__device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_out) {
+__device__ bool maybe_shift(const Dom& a, Red& red, StepState& st, int& rows_out) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     rows_out = 0;
@@ -1068,7 +1086,7 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     double v1[1] = {local};
     if (!red.reduce<1>(v1, kMax, kTagShift)) return false;
     const double front = v1[0];
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.B.ctl->out[0] = front;
+    if (a.bid == 0 && threadIdx.x == 0) a.B.ctl->out[0] = front;
     if (front < a.shift_trigger) return true;
     const int rows = (int)floor((front - a.shift_target) / P.dy);
     double gmax = 0;
@@ -1082,11 +1100,11 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     double v2[1] = {gmax};
     if (!red.reduce<1>(v2, kMax, kTagShift)) return false;
     if (v2[0] > 1e-6) {
-        set_error(B.ctl, PEARL_ERR_UNSAFE_SHIFT, 0);
+        set_error(a, PEARL_ERR_UNSAFE_SHIFT, 0);
         return false;
     }
     if (rows <= 0 || rows >= P.ny || a.shift_c_gamma < 0 || a.shift_c_gamma > 1) {
-        set_error(B.ctl, PEARL_ERR_INVALID_ARGUMENT, 0);
+        set_error(a, PEARL_ERR_INVALID_ARGUMENT, 0);
         return false;
     }
     const int nw = cur ^ 1;
@@ -1124,11 +1142,11 @@ __device__ bool maybe_shift(const KArgs& a, Red& red, StepState& st, int& rows_o
     double v3[3] = {removed, vmix, vnonfin};
     if (!red.reduce<3>(v3, OPS3(kSum, kMax, kMax), kTagShift)) return false;
     if (v3[1] != 0) {
-        set_error(B.ctl, PEARL_ERR_MIXTURE, 0);
+        set_error(a, PEARL_ERR_MIXTURE, 0);
         return false;
     }
     if (v3[2] != 0) {
-        set_error(B.ctl, PEARL_ERR_NONFINITE_CARBON, 0);
+        set_error(a, PEARL_ERR_NONFINITE_CARBON, 0);
         return false;
     }
     const double added = rows * P.nx * a.shift_c_gamma * P.dx * P.dy;
@@ -1167,7 +1185,7 @@ __device__ __forceinline__ double interface_energy_cell(const DevParams& P, cons
 
 // Interface-only energy of state set `s` plus its phase-fraction sums.
 // Reduction: {energy sum, sum phi_alpha, sum phi_theta, sum phi_gamma}.
-__device__ bool phase_interface_energy(const KArgs& a, Red& red, int s, double& energy, double* frac) {
+__device__ bool phase_interface_energy(const Dom& a, Red& red, int s, double& energy, double* frac) {
     const DevParams& P = a.P;
     const double* const* ph = a.B.phi[s];
     double ven = 0, f0 = 0, f1 = 0, f2 = 0;
@@ -1196,7 +1214,7 @@ __device__ bool phase_interface_energy(const KArgs& a, Red& red, int s, double& 
 
 // Capillary force of smooth_interface_only (pearl_serial.cpp:892-917) written
 // to the work planes x, r, z; reduction {max |force|}.
-__device__ bool phase_smooth_force(const KArgs& a, Red& red, int cur, double& force_max) {
+__device__ bool phase_smooth_force(const Dom& a, Red& red, int cur, double& force_max) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const double* const* ph = B.phi[cur];
@@ -1252,7 +1270,7 @@ __device__ bool phase_smooth_force(const KArgs& a, Red& red, int cur, double& fo
 // Backtracking trial of smooth_interface_only (pearl_serial.cpp:925-933):
 // trial phi = project(phi - scale*force) into set cur^1.
 // Reduction: {max |dphi|, simplex failed}.
-__device__ bool phase_smooth_trial(const KArgs& a, Red& red, int cur, double scale, double& change, bool& bad) {
+__device__ bool phase_smooth_trial(const Dom& a, Red& red, int cur, double scale, double& change, bool& bad) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const double* const* ph = B.phi[cur];
@@ -1285,7 +1303,7 @@ __device__ bool phase_smooth_trial(const KArgs& a, Red& red, int cur, double sca
 // current state.  Report layout in ctl->out: steps, converged, energy_initial,
 // energy_final, final_relative_energy_change, final_max_phase_change,
 // phase fractions before (3) and after (3).
-__device__ bool smooth(const KArgs& a, Red& red, StepState& st, double* rep) {
+__device__ bool smooth(const Dom& a, Red& red, StepState& st, double* rep) {
     const DevParams& P = a.P;
     Ctl* ctl = a.B.ctl;
     const int max_steps = a.smooth_max_steps, min_steps = a.smooth_min_steps;
@@ -1305,7 +1323,7 @@ __device__ bool smooth(const KArgs& a, Red& red, StepState& st, double* rep) {
         double force_max;
         if (!phase_smooth_force(a, red, st.cur, force_max)) return false;
         if (!isfinite(force_max)) {
-            set_error(ctl, PEARL_ERR_SMOOTHING, 1);
+            set_error(a, PEARL_ERR_SMOOTHING, 1);
             return false;
         }
         if (force_max == 0) {
@@ -1322,7 +1340,7 @@ __device__ bool smooth(const KArgs& a, Red& red, StepState& st, double* rep) {
             bool bad;
             if (!phase_smooth_trial(a, red, st.cur, scale, actual_change, bad)) return false;
             if (bad) {
-                set_error(ctl, PEARL_ERR_SIMPLEX, 0);
+                set_error(a, PEARL_ERR_SIMPLEX, 0);
                 return false;
             }
             double f3[3];
@@ -1337,7 +1355,7 @@ __device__ bool smooth(const KArgs& a, Red& red, StepState& st, double* rep) {
                 scale *= .5;
         }
         if (!accepted) {
-            set_error(ctl, PEARL_ERR_SMOOTHING, 2);
+            set_error(a, PEARL_ERR_SMOOTHING, 2);
             return false;
         }
         st.cur ^= 1;  // only the phase planes of the new set are meaningful here
@@ -1367,7 +1385,7 @@ __device__ bool smooth(const KArgs& a, Red& red, StepState& st, double* rep) {
 
 // Sums of the mixture intercept and susceptibility (the mean_carbon solve of
 // initialize, pearl_serial.cpp:1814-1822).  Reduction: {sum c0, sum chi, invalid}.
-__device__ bool phase_mix_sums(const KArgs& a, Red& red, int s, double& si, double& sc, bool& mixbad) {
+__device__ bool phase_mix_sums(const Dom& a, Red& red, int s, double& si, double& sc, bool& mixbad) {
     const DevParams& P = a.P;
     const double* const* ph = a.B.phi[s];
     double v0 = 0, v1 = 0, vb = 0;
@@ -1392,7 +1410,7 @@ __device__ bool phase_mix_sums(const KArgs& a, Red& red, int s, double& si, doub
 
 // Uniform mu and the carbon it implies (initialize, pearl_serial.cpp:1823-1826).
 // Reduction: {sum carbon, invalid}.
-__device__ bool phase_init_composition(const KArgs& a, Red& red, int s, double mu, double& mass, bool& mixbad) {
+__device__ bool phase_init_composition(const Dom& a, Red& red, int s, double mu, double& mass, bool& mixbad) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const double* const* ph = B.phi[s];
@@ -1418,7 +1436,7 @@ __device__ bool phase_init_composition(const KArgs& a, Red& red, int s, double m
 }
 
 // snapshot() reductions (pearl_serial.cpp:2266-2281) on state `s`.
-__device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
+__device__ bool snapshot(const Dom& a, Red& red, int s, double* out) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
     const double* const* ph = B.phi[s];
@@ -1442,7 +1460,10 @@ __device__ bool snapshot(const KArgs& a, Red& red, int s, double* out) {
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs args) {
+    const Dom a{args.P, args.B, args.maps, args.use_tma, (int)blockIdx.x, (int)gridDim.x, args.B.ctl, args.B.part,
+                args.shift_trigger, args.shift_target, args.shift_c_gamma, args.smooth_max_steps,
+                args.smooth_min_steps, args.smooth_energy_rtol, args.smooth_max_phase_change};
     Ctl* ctl = a.B.ctl;
     __shared__ PhaseClock clk;
     extern __shared__ __align__(128) unsigned char dsmem[];
@@ -1464,24 +1485,24 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
     st.mass0 = ctl->mass0;
     const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
 
-    if (a.mode == kModeRun) {
+    if (args.mode == kModeRun) {
         long long steps = 0, cg_total = 0;
         int cg_peak = 0, reached = 0;
         pearl_step_info last;
         memset(&last, 0, sizeof last);
-        while (steps < a.L.max_steps) {
-            if (!(st.S.time < a.L.end_time)) break;
-            if (st.S.step >= a.L.config_max_steps) {
-                set_error(ctl, PEARL_ERR_MAX_STEPS, 0);
+        while (steps < args.L.max_steps) {
+            if (!(st.S.time < args.L.end_time)) break;
+            if (st.S.step >= args.L.config_max_steps) {
+                set_error(a, PEARL_ERR_MAX_STEPS, 0);
                 break;
             }
             pearl_step_info info;
-            if (!advance(a, red, st, a.L.stop_time, info)) break;
+            if (!advance(a, red, st, args.L.stop_time, info)) break;
             ++steps;
             cg_total += info.cg_iterations;
             cg_peak = info.cg_iterations > cg_peak ? info.cg_iterations : cg_peak;
             last = info;
-            if (st.S.time >= a.L.stop_time - a.L.output_eps) {
+            if (st.S.time >= args.L.stop_time - args.L.output_eps) {
                 reached = 1;
                 break;
             }
@@ -1501,10 +1522,10 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModePropose) {
+    if (args.mode == kModePropose) {
         double change;
         bool mixbad, simplexbad;
-        if (!phase_propose(a, red, st.cur, a.dt, change, mixbad, simplexbad)) return;
+        if (!phase_propose(a, red, st.cur, args.dt, change, mixbad, simplexbad)) return;
         if (leader) {
             ctl->out[0] = change;
             ctl->iout[0] = mixbad;
@@ -1513,16 +1534,16 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeMix) {
+    if (args.mode == kModeMix) {
         bool mixbad;
         if (!phase_mix(a, red, st.cur, mixbad)) return;
         if (leader) ctl->iout[0] = mixbad;
         red.flush();
         return;
     }
-    if (a.mode == kModeDiffusion) {
+    if (args.mode == kModeDiffusion) {
         DiffusionOut d;
-        if (!diffusion(a, red, st.cur, a.dt, d)) return;
+        if (!diffusion(a, red, st.cur, args.dt, d)) return;
         if (leader) {
             ctl->iout[0] = d.ok;
             ctl->iout[1] = d.it;
@@ -1532,7 +1553,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeEnergy || a.mode == kModeValid) {
+    if (args.mode == kModeEnergy || args.mode == kModeValid) {
         double e, m;
         bool mixbad, bad;
         if (!phase_energy(a, red, st.cur, e, m, mixbad, bad)) return;
@@ -1545,7 +1566,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeSnapshot) {
+    if (args.mode == kModeSnapshot) {
         double v[5];
         if (!snapshot(a, red, st.cur, v)) return;
         double e, m;
@@ -1560,7 +1581,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeSmooth) {
+    if (args.mode == kModeSmooth) {
         double rep[12];
         if (!smooth(a, red, st, rep)) return;
         if (leader) {
@@ -1571,7 +1592,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeMixSums) {
+    if (args.mode == kModeMixSums) {
         double si, sc;
         bool mixbad;
         if (!phase_mix_sums(a, red, st.cur, si, sc, mixbad)) return;
@@ -1583,10 +1604,10 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeInitComposition) {
+    if (args.mode == kModeInitComposition) {
         double mass;
         bool mixbad;
-        if (!phase_init_composition(a, red, st.cur, a.init_mu, mass, mixbad)) return;
+        if (!phase_init_composition(a, red, st.cur, args.init_mu, mass, mixbad)) return;
         if (leader) {
             ctl->out[0] = mass;
             ctl->iout[0] = mixbad;
@@ -1595,7 +1616,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         red.flush();
         return;
     }
-    if (a.mode == kModeMaybeShift) {
+    if (args.mode == kModeMaybeShift) {
         int rows = 0;
         if (!maybe_shift(a, red, st, rows)) return;
         if (leader) {
@@ -1606,6 +1627,115 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
         }
         red.flush();
         return;
+    }
+}
+
+// ------------------------------------------------------------------ batched instances
+// A batch advances many independent instances (own grid size, parameters,
+// dt, retries and CG count) in one cooperative launch.  The grid is split
+// into groups of `group_blocks` blocks; each group runs the same `advance`
+// device code on its own list of instances, one after another, with barriers
+// and reductions local to the group.
+struct alignas(64) BatchInstance {
+    CUtensorMap maps[kMapCount];
+    DevParams P;
+    DevBufs B;  // B.ctl: the instance's control block; B.part: unused
+};
+
+struct BatchArgs {
+    const BatchInstance* inst;
+    const int* order;  // instance ids grouped by block group
+    const int* first;  // group g owns order[first[g] .. first[g+1])
+    int group_blocks;
+    Ctl* group_ctl;      // [groups] barrier words and error status
+    double* group_part;  // [groups][2][group_blocks][kMaxRed]
+    int use_tma;
+    pearl_run_limits L;
+};
+
+__global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
+    const int g = blockIdx.x / args.group_blocks, bid = blockIdx.x % args.group_blocks;
+    __shared__ PhaseClock clk;
+    __shared__ DevParams sP;
+    __shared__ DevBufs sB;
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    Pipe pipe{reinterpret_cast<uint64_t*>(dsmem), reinterpret_cast<double*>(dsmem + 128), 0u};
+    if (args.use_tma) {
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < kMaxStages; ++s) mbar_init(&pipe.bar[s], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
+    Ctl* gctl = args.group_ctl + g;
+    double* gpart = args.group_part + (size_t)g * 2 * args.group_blocks * kMaxRed;
+    const bool leader = bid == 0 && threadIdx.x == 0;
+    for (int j = args.first[g]; j < args.first[g + 1]; ++j) {
+        const BatchInstance* I = args.inst + args.order[j];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sP = I->P;
+            sB = I->B;
+        }
+        __syncthreads();
+        const Dom a{sP, sB, I->maps, args.use_tma, bid, args.group_blocks, gctl, gpart, 0, 0, 0, 0, 0, 0, 0};
+        Red red(a, &clk);
+        red.pipe_ptr = &pipe;
+        Ctl* ctl = sB.ctl;
+        StepState st;
+        st.S = ctl->S;
+        st.cur = ctl->cur;
+        st.cache_valid = ctl->energy_valid != 0;
+        st.e0 = ctl->e0;
+        st.mass0 = ctl->mass0;
+        long long steps = 0, cg_total = 0;
+        int cg_peak = 0, reached = 0;
+        pearl_step_info last;
+        memset(&last, 0, sizeof last);
+        bool failed = false;
+        while (steps < args.L.max_steps) {
+            if (!(st.S.time < args.L.end_time)) break;
+            if (st.S.step >= args.L.config_max_steps) {
+                set_error(a, PEARL_ERR_MAX_STEPS, 0);
+                failed = true;
+                break;
+            }
+            pearl_step_info info;
+            if (!advance(a, red, st, args.L.stop_time, info)) {
+                failed = true;
+                break;
+            }
+            ++steps;
+            cg_total += info.cg_iterations;
+            cg_peak = info.cg_iterations > cg_peak ? info.cg_iterations : cg_peak;
+            last = info;
+            if (st.S.time >= args.L.stop_time - args.L.output_eps) {
+                reached = 1;
+                break;
+            }
+        }
+        // a bounded wait that ran out leaves the group's barrier unusable: stop
+        if (failed && *(volatile int*)&gctl->status == PEARL_ERR_DEVICE_WAIT) {
+            if (leader) ctl->status = PEARL_ERR_DEVICE_WAIT;
+            return;
+        }
+        if (leader) {
+            ctl->S = st.S;
+            ctl->cur = st.cur;
+            ctl->energy_valid = st.cache_valid ? 1 : 0;
+            ctl->e0 = st.e0;
+            ctl->mass0 = st.mass0;
+            ctl->steps = steps;
+            ctl->cg_total = cg_total;
+            ctl->cg_peak = cg_peak;
+            ctl->reached_stop = reached;
+            ctl->last = last;
+            ctl->status = failed ? gctl->status : 0;
+            ctl->why = failed ? gctl->why : 0;
+            gctl->status = 0;
+            gctl->why = 0;
+        }
+        red.flush();
     }
 }
 
@@ -1888,8 +2018,14 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
     return true;
 }
 
+int ensure_stage(pearl_gpu_ctx* ctx) {
+    if (!ctx->h_stage) PG_CUDA(ctx, cudaMallocHost(&ctx->h_stage, ctx->stage_elems * sizeof(double)));
+    return PEARL_OK;
+}
+
 // AoS host (ny,nx,3) + two scalar fields <-> padded SoA device planes
 int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* carbon, const double* mu) {
+    if (int rc = ensure_stage(ctx)) return rc;
     const size_t n = (size_t)ctx->nx * ctx->ny;
     const size_t pe = plane_elems(ctx);
     double* st = ctx->h_stage;
@@ -1922,6 +2058,7 @@ int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* car
 }
 
 int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, double* mu) {
+    if (int rc = ensure_stage(ctx)) return rc;
     const size_t pe = plane_elems(ctx);
     double* st = ctx->h_stage;
     if (phi)
@@ -2044,8 +2181,7 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     std::memset(ctx->h_ctl, 0, sizeof(Ctl));
     ctx->B.ctl = ctx->d_ctl;
     if (ctx->use_tma && !build_tensor_maps(ctx)) ctx->use_tma = false;
-    ctx->stage_elems = 5 * pe;
-    if (cudaMallocHost(&ctx->h_stage, ctx->stage_elems * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
+    ctx->stage_elems = 5 * pe;  // pinned staging is allocated at the first host transfer
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
         return bail(PEARL_ERR_CUDA);
     if (cudaMemcpy(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -2349,6 +2485,309 @@ int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* launches, int* grid_blo
     if (last_ms) *last_ms = ctx->last_ms;
     return PEARL_OK;
 }
+
+}  // extern "C"
+
+// ============================================================ batched instances
+struct pearl_gpu_batch {
+    int device = 0, n = 0;
+    std::vector<pearl_gpu_ctx*> inst;  // host bookkeeping and buffers of every instance
+    Ctl* d_ctls = nullptr;             // the instances' control blocks, contiguous
+    Ctl* h_ctls = nullptr;             // pinned mirror
+    BatchInstance* d_inst = nullptr;
+    int* d_order = nullptr;
+    int* d_first = nullptr;
+    Ctl* d_group_ctl = nullptr;
+    double* d_group_part = nullptr;
+    int per_sm = 0, sms = 0, grid = 0, group_blocks = 0, ngroups = 0;
+    bool use_tma = true;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+    long long launches = 0;
+    std::string error;
+};
+
+namespace {
+
+int bfail(pearl_gpu_batch* b, int status, const std::string& msg) {
+    if (b) b->error = msg;
+    return status;
+}
+#define PB_CUDA(b, call)                                                                        \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return bfail(b, PEARL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Split the cooperative grid into groups of `gb` blocks and hand out the
+// instances longest-first to the least-loaded group (cost ~ cells).
+int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma) {
+    const int max_grid = b->per_sm * b->sms;
+    if (gb < 1 || gb > max_grid) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid group size");
+    b->group_blocks = gb;
+    b->ngroups = max_grid / gb;
+    b->grid = b->ngroups * gb;
+    b->use_tma = use_tma;
+    std::vector<int> idx(b->n);
+    for (int i = 0; i < b->n; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](int x, int y) {
+        return (long long)b->inst[x]->nx * b->inst[x]->ny > (long long)b->inst[y]->nx * b->inst[y]->ny;
+    });
+    std::vector<double> load(b->ngroups, 0.0);
+    std::vector<std::vector<int>> lists(b->ngroups);
+    for (int i : idx) {
+        // a group's blocks share an instance's tiles: cost = cells / min(blocks, tiles)
+        const pearl_gpu_ctx* c = b->inst[i];
+        const double cells = (double)c->nx * c->ny;
+        const double cost = cells / std::max(1, std::min(gb, c->P.ntiles));
+        int best = 0;
+        for (int g = 1; g < b->ngroups; ++g)
+            if (load[g] < load[best]) best = g;
+        load[best] += cost;
+        lists[best].push_back(i);
+    }
+    std::vector<int> order, first(1, 0);
+    for (int g = 0; g < b->ngroups; ++g) {
+        order.insert(order.end(), lists[g].begin(), lists[g].end());
+        first.push_back((int)order.size());
+    }
+    cudaFree(b->d_order);
+    cudaFree(b->d_first);
+    cudaFree(b->d_group_ctl);
+    cudaFree(b->d_group_part);
+    b->d_order = nullptr;
+    b->d_first = nullptr;
+    b->d_group_ctl = nullptr;
+    b->d_group_part = nullptr;
+    PB_CUDA(b, cudaMalloc(&b->d_order, sizeof(int) * std::max(1, b->n)));
+    PB_CUDA(b, cudaMalloc(&b->d_first, sizeof(int) * first.size()));
+    PB_CUDA(b, cudaMalloc(&b->d_group_ctl, sizeof(Ctl) * b->ngroups));
+    PB_CUDA(b, cudaMalloc(&b->d_group_part, sizeof(double) * (size_t)b->ngroups * 2 * gb * kMaxRed));
+    PB_CUDA(b, cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+    PB_CUDA(b, cudaMemcpy(b->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+    PB_CUDA(b, cudaMemset(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups));
+    // per-instance descriptors (tensor maps, parameters, buffers)
+    std::vector<BatchInstance> hi(b->n);
+    for (int i = 0; i < b->n; ++i) {
+        std::memcpy(hi[i].maps, b->inst[i]->maps, sizeof hi[i].maps);
+        hi[i].P = b->inst[i]->P;
+        hi[i].B = b->inst[i]->B;
+    }
+    PB_CUDA(b, cudaMemcpy(b->d_inst, hi.data(), sizeof(BatchInstance) * b->n, cudaMemcpyHostToDevice));
+    return PEARL_OK;
+}
+
+int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
+    PB_CUDA(b, cudaSetDevice(b->device));
+    PB_CUDA(b, cudaMemsetAsync(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups, b->stream));
+    BatchArgs args{};
+    args.inst = b->d_inst;
+    args.order = b->d_order;
+    args.first = b->d_first;
+    args.group_blocks = b->group_blocks;
+    args.group_ctl = b->d_group_ctl;
+    args.group_part = b->d_group_part;
+    args.use_tma = b->use_tma ? 1 : 0;
+    args.L = L;
+    void* kargs[] = {&args};
+    PB_CUDA(b, cudaEventRecord(b->ev0, b->stream));
+    PB_CUDA(b, cudaLaunchCooperativeKernel((const void*)pearl_batch_kernel, dim3(b->grid), dim3(kThreads), kargs,
+                                           b->use_tma ? kTmaSmemBytes : 0, b->stream));
+    b->launches++;
+    PB_CUDA(b, cudaEventRecord(b->ev1, b->stream));
+    PB_CUDA(b, cudaMemcpyAsync(b->h_ctls, b->d_ctls, sizeof(Ctl) * b->n, cudaMemcpyDeviceToHost, b->stream));
+    PB_CUDA(b, cudaStreamSynchronize(b->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->last_ms = ms;
+    for (int i = 0; i < b->n; ++i) *b->inst[i]->h_ctl = b->h_ctls[i];
+    return PEARL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pearl_gpu_batch_destroy(pearl_gpu_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto* c : b->inst) {
+        if (c) c->d_ctl = nullptr;  // owned by the batch
+        pearl_gpu_destroy(c);
+    }
+    cudaFree(b->d_ctls);
+    if (b->h_ctls) cudaFreeHost(b->h_ctls);
+    cudaFree(b->d_inst);
+    cudaFree(b->d_order);
+    cudaFree(b->d_first);
+    cudaFree(b->d_group_ctl);
+    cudaFree(b->d_group_part);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    delete b;
+}
+
+int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, const int* ny, int device,
+                           int group_blocks, pearl_gpu_batch** out) {
+    if (!out || n < 1 || !params || !nx || !ny) return PEARL_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    pearl_gpu_batch* b = new pearl_gpu_batch();
+    b->device = device;
+    b->n = n;
+    auto bail = [&](int rc) {
+        pearl_gpu_batch_destroy(b);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(PEARL_ERR_NO_DEVICE);
+    b->inst.assign(n, nullptr);
+    if (cudaMalloc(&b->d_ctls, sizeof(Ctl) * n) != cudaSuccess ||
+        cudaMallocHost(&b->h_ctls, sizeof(Ctl) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_inst, sizeof(BatchInstance) * n) != cudaSuccess)
+        return bail(PEARL_ERR_CUDA);
+    std::memset(b->h_ctls, 0, sizeof(Ctl) * n);
+    bool tma = true;
+    for (int i = 0; i < n; ++i) {
+        const int rc = pearl_gpu_create(&params[i], nx[i], ny[i], device, &b->inst[i]);
+        if (rc) return bail(rc);
+        pearl_gpu_ctx* c = b->inst[i];
+        cudaFree(c->d_ctl);  // the batch keeps every control block in one array
+        c->d_ctl = b->d_ctls + i;
+        c->B.ctl = c->d_ctl;
+        if (cudaMemcpy(c->d_ctl, c->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(PEARL_ERR_CUDA);
+        tma = tma && c->use_tma;
+    }
+    if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return bail(PEARL_ERR_CUDA);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+    if (tma &&
+        cudaFuncSetAttribute(pearl_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
+            cudaSuccess)
+        tma = false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->per_sm, pearl_batch_kernel, kThreads,
+                                                      tma ? kTmaSmemBytes : 0) != cudaSuccess ||
+        b->per_sm < 1)
+        return bail(PEARL_ERR_CUDA);
+    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : 4, tma);
+    if (rc) return bail(rc);
+    *out = b;
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_upload(pearl_gpu_batch* b, int i, const double* phi, const double* carbon, const double* mu,
+                           const pearl_scalars* scalars) {
+    if (!b || i < 0 || i >= b->n) return PEARL_ERR_INVALID_ARGUMENT;
+    const int rc = pearl_gpu_upload(b->inst[i], phi, carbon, mu, scalars);
+    if (rc) return bfail(b, rc, pearl_gpu_last_error(b->inst[i]));
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_download(pearl_gpu_batch* b, int i, double* phi, double* carbon, double* mu,
+                             pearl_scalars* scalars) {
+    if (!b || i < 0 || i >= b->n) return PEARL_ERR_INVALID_ARGUMENT;
+    const int rc = pearl_gpu_download(b->inst[i], phi, carbon, mu, scalars);
+    if (rc) return bfail(b, rc, pearl_gpu_last_error(b->inst[i]));
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_run(pearl_gpu_batch* b, const pearl_run_limits* limits, pearl_run_report* reports,
+                        int* status) {
+    if (!b || !limits || limits->max_steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
+    int rc = batch_launch(b, *limits);
+    if (rc) return rc;
+    int first_bad = PEARL_OK;
+    for (int i = 0; i < b->n; ++i) {
+        const Ctl& h = b->h_ctls[i];
+        if (reports) {
+            reports[i].steps = h.steps;
+            reports[i].cg_total = h.cg_total;
+            reports[i].cg_peak = h.cg_peak;
+            reports[i].reached_stop = h.reached_stop;
+            reports[i].last = h.last;
+        }
+        if (status) status[i] = h.status;
+        if (h.status == PEARL_ERR_DEVICE_WAIT) first_bad = PEARL_ERR_DEVICE_WAIT;
+    }
+    if (first_bad) return bfail(b, first_bad, "device grid barrier wait exceeded its limit");
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, int* use_tma) {
+    if (!b || steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
+    PB_CUDA(b, cudaSetDevice(b->device));
+    // back up every instance's current state (5 planes) and control block
+    std::vector<double*> backup(b->n, nullptr);
+    auto release = [&]() {
+        for (double* p : backup) cudaFree(p);
+    };
+    for (int i = 0; i < b->n; ++i) {
+        pearl_gpu_ctx* c = b->inst[i];
+        const size_t bytes = 5 * plane_elems(c) * sizeof(double);
+        if (cudaMalloc(&backup[i], bytes) != cudaSuccess) {
+            release();
+            return bfail(b, PEARL_ERR_CUDA, "autotune backup allocation");
+        }
+        cudaMemcpyAsync(backup[i], c->B.phi[c->h_ctl->cur][0], bytes, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    // the instances' host control blocks are authoritative (uploads update them)
+    std::vector<Ctl> saved(b->n);
+    for (int i = 0; i < b->n; ++i) saved[i] = *b->inst[i]->h_ctl;
+    const bool can_tma = b->use_tma;
+    double best_ms = 1e300;
+    int best_gb = b->group_blocks;
+    bool best_tma = b->use_tma;
+    const int cands[] = {1, 2, 4, 8, 16};
+    pearl_run_limits L{1, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
+    for (int tma = can_tma ? 1 : 0; tma >= 0; --tma) {
+        for (int gb : cands) {
+            if (gb > b->per_sm * b->sms) continue;
+            int rc = batch_configure(b, gb, tma != 0);
+            double ms = 0;
+            for (int s = 0; rc == PEARL_OK && s < steps; ++s) {
+                rc = batch_launch(b, L);
+                ms += b->last_ms;
+            }
+            // restore
+            for (int i = 0; i < b->n; ++i) {
+                pearl_gpu_ctx* c = b->inst[i];
+                cudaMemcpyAsync(c->B.phi[saved[i].cur][0], backup[i], 5 * plane_elems(c) * sizeof(double),
+                                cudaMemcpyDeviceToDevice, b->stream);
+            }
+            std::memcpy(b->h_ctls, saved.data(), sizeof(Ctl) * b->n);
+            cudaMemcpyAsync(b->d_ctls, b->h_ctls, sizeof(Ctl) * b->n, cudaMemcpyHostToDevice, b->stream);
+            cudaStreamSynchronize(b->stream);
+            for (int i = 0; i < b->n; ++i) *b->inst[i]->h_ctl = saved[i];
+            if (rc) {
+                release();
+                return rc;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_gb = gb;
+                best_tma = tma != 0;
+            }
+        }
+    }
+    release();
+    const int rc = batch_configure(b, best_gb, best_tma);
+    if (group_blocks) *group_blocks = best_gb;
+    if (use_tma) *use_tma = best_tma ? 1 : 0;
+    return rc;
+}
+
+int pearl_gpu_batch_stats(const pearl_gpu_batch* b, long long* launches, int* grid_blocks, int* group_blocks,
+                          double* last_kernel_ms) {
+    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
+    if (launches) *launches = b->launches;
+    if (grid_blocks) *grid_blocks = b->grid;
+    if (group_blocks) *group_blocks = b->group_blocks;
+    if (last_kernel_ms) *last_kernel_ms = b->last_ms;
+    return PEARL_OK;
+}
+
+const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* b) { return b ? b->error.c_str() : "null batch"; }
 
 }  // extern "C"
 

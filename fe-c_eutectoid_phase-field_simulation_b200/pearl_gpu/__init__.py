@@ -115,7 +115,9 @@ EXPORTS = [
     "pearl_gpu_implicit_diffusion", "pearl_gpu_download_trial", "pearl_gpu_energy_mass", "pearl_gpu_valid_state",
     "pearl_gpu_status_string", "pearl_gpu_last_error", "pearl_gpu_stats", "pearl_gpu_phase_times",
     "pearl_gpu_selftest_division", "pearl_gpu_advance_noalloc", "pearl_gpu_smooth_interface",
-    "pearl_gpu_mixture_sums", "pearl_gpu_init_composition",
+    "pearl_gpu_mixture_sums", "pearl_gpu_init_composition", "pearl_gpu_batch_create", "pearl_gpu_batch_destroy",
+    "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
+    "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error",
 ]
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
@@ -165,6 +167,17 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_init_composition.argtypes = [V, D, DP]
     L.pearl_gpu_advance_noalloc.argtypes = [C.POINTER(PearlParams), C.c_int, C.c_int, V, V, V,
                                             C.POINTER(PearlScalars), D, C.POINTER(PearlStepInfo), V]
+    IP = C.POINTER(C.c_int)
+    L.pearl_gpu_batch_create.argtypes = [C.c_int, C.POINTER(PearlParams), IP, IP, C.c_int, C.c_int, C.POINTER(V)]
+    L.pearl_gpu_batch_destroy.argtypes = [V]
+    L.pearl_gpu_batch_destroy.restype = None
+    L.pearl_gpu_batch_upload.argtypes = [V, C.c_int, DP, DP, DP, C.POINTER(PearlScalars)]
+    L.pearl_gpu_batch_download.argtypes = [V, C.c_int, DP, DP, DP, C.POINTER(PearlScalars)]
+    L.pearl_gpu_batch_run.argtypes = [V, C.POINTER(PearlRunLimits), C.POINTER(PearlRunReport), IP]
+    L.pearl_gpu_batch_autotune.argtypes = [V, C.c_int, IP, IP]
+    L.pearl_gpu_batch_stats.argtypes = [V, C.POINTER(C.c_longlong), IP, IP, DP]
+    L.pearl_gpu_batch_last_error.argtypes = [V]
+    L.pearl_gpu_batch_last_error.restype = C.c_char_p
     if path is None:
         _lib = L
     return L
@@ -339,3 +352,82 @@ class Context:
         n, g, ms = C.c_longlong(), C.c_int(), D()
         self._check(self.lib.pearl_gpu_stats(self.h, C.byref(n), C.byref(g), C.byref(ms)))
         return dict(launches=n.value, grid=g.value, last_ms=ms.value)
+
+
+class Batch:
+    """Many independent domains advanced in one persistent launch (pearl_gpu_batch).
+
+    ``cases`` is a sequence of (params, nx, ny).  Each instance follows the
+    same step path as a :class:`Context` of its own.
+    """
+
+    def __init__(self, cases, device: int = 0, group_blocks: int = 0):
+        self.lib = library()
+        self.n = len(cases)
+        self.shapes = [(int(nx), int(ny)) for _, nx, ny in cases]
+        prm = (PearlParams * self.n)()
+        for i, (p, _, _) in enumerate(cases):
+            prm[i] = p if isinstance(p, PearlParams) else PearlParams.from_dict(p)
+        nx = (C.c_int * self.n)(*[s[0] for s in self.shapes])
+        ny = (C.c_int * self.n)(*[s[1] for s in self.shapes])
+        h = C.c_void_p()
+        rc = self.lib.pearl_gpu_batch_create(self.n, prm, nx, ny, device, group_blocks, C.byref(h))
+        if rc:
+            raise PearlError(rc, f"pearl_gpu_batch_create failed: {STATUS.get(rc, rc)}")
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            raise PearlError(rc, self.lib.pearl_gpu_batch_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.pearl_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def upload(self, i: int, phi, carbon, mu, scalars: dict | PearlScalars | None = None) -> None:
+        s = None
+        if scalars is not None:
+            s = scalars if isinstance(scalars, PearlScalars) else PearlScalars.from_dict(scalars)
+        self._check(self.lib.pearl_gpu_batch_upload(self.h, i, _p(phi), _p(carbon), _p(mu),
+                                                    C.byref(s) if s else None))
+
+    def download(self, i: int):
+        nx, ny = self.shapes[i]
+        phi = np.empty((ny, nx, 3))
+        carbon = np.empty((ny, nx))
+        mu = np.empty((ny, nx))
+        s = PearlScalars()
+        self._check(self.lib.pearl_gpu_batch_download(self.h, i, _p(phi), _p(carbon), _p(mu), C.byref(s)))
+        return phi, carbon, mu, s
+
+    def run(self, max_steps: int, stop_time: float = 1e300, end_time: float = 1e300, output_eps: float = 0.0,
+            config_max_steps: int = 2**62):
+        """Returns (reports, statuses), one entry per instance."""
+        lim = PearlRunLimits(max_steps, config_max_steps, stop_time, end_time, output_eps)
+        reps = (PearlRunReport * self.n)()
+        st = (C.c_int * self.n)()
+        self._check(self.lib.pearl_gpu_batch_run(self.h, C.byref(lim), reps, st))
+        return list(reps), list(st)
+
+    def autotune(self, steps: int = 2):
+        g, t = C.c_int(), C.c_int()
+        self._check(self.lib.pearl_gpu_batch_autotune(self.h, steps, C.byref(g), C.byref(t)))
+        return g.value, bool(t.value)
+
+    def stats(self):
+        n, grid, gb, ms = C.c_longlong(), C.c_int(), C.c_int(), D()
+        self._check(self.lib.pearl_gpu_batch_stats(self.h, C.byref(n), C.byref(grid), C.byref(gb), C.byref(ms)))
+        return dict(launches=n.value, grid=grid.value, group_blocks=gb.value, last_ms=ms.value)

@@ -221,3 +221,26 @@ def scaled(nx: int, ny: int, seed: int = 0, undercooling: float = 10.0, dt: floa
     fronts = front + (rng.integers(-front_jitter, front_jitter + 1, size=nx) if front_jitter else 0.0)
     phi = lamellar_phi(nx, ny, widths, thetas, np.broadcast_to(fronts, (nx,)))
     return _finish(f"scaled_{nx}x{ny}", nx, ny, params, phi, dict(dt=dt, seed=seed, pairs=pairs))
+
+
+def sweep_instance(i: int, rng: np.random.Generator, dt: float = 4e-12) -> Workload:
+    """One instance of the parameter sweep: 2 lamellar pairs of spacing U{16..96}
+    cells across x (nx = 2 spacings), growth length ny = U{64..1024} cells,
+    ferrite fraction U(0.85, 0.90), undercooling U(5, 40) K, adaptive dt."""
+    spacing = int(rng.integers(16, 97))
+    ny = int(rng.integers(64, 1025))
+    ferrite = float(rng.uniform(0.85, 0.90))
+    undercooling = float(rng.uniform(5.0, 40.0))
+    nx = 2 * spacing
+    dx = 2e-9
+    params = make_params(nx, ny, dx, undercooling=undercooling, dt=dt, dt_max=2 * dt)
+    widths, thetas = jittered_pairs(nx, 2, rng, 0.0, ferrite)
+    phi = lamellar_phi(nx, ny, widths, thetas, np.full(nx, 32.0))
+    meta = dict(dt=dt, index=i, spacing=spacing, ferrite_fraction=ferrite, undercooling=undercooling)
+    return _finish(f"sweep_{i}_{nx}x{ny}", nx, ny, params, phi, meta)
+
+
+def sweep(n: int = 256, seed: int = 0) -> list[Workload]:
+    """n sweep instances drawn from one seed (the batched-sweep workload)."""
+    rng = np.random.default_rng(seed)
+    return [sweep_instance(i, rng) for i in range(n)]

@@ -199,9 +199,11 @@ const char* pearl_gpu_last_error(const pearl_gpu_ctx* ctx);
 int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* kernel_launches, int* grid_blocks, double* last_kernel_ms);
 /* Device time of the last launch split by phase (16 slots, milliseconds and
  * phase counts): 0 propose, 1 diffusion set-up, 2 CG apply, 3 CG update,
- * 4 true residual, 5 CG restart, 6 diffusion final + acceptance reductions,
+ * 4 unused (the true-residual recheck runs inside slot 6), 5 CG restart,
+ * 6 diffusion final (true residual, closure, mu, acceptance reductions),
  * 7 step-start energy, 8 phase-only final, 9 mixture, 10 moving window,
- * 11 snapshot.  Each slot covers its sweep, reduction and grid barrier. */
+ * 11 snapshot, 12 interface smoothing, 13 initial composition.  Each slot
+ * covers its sweep, reduction and grid barrier. */
 int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts);
 
 /* Self-test of the device's exact division by a precomputed reciprocal, which
@@ -224,7 +226,7 @@ int pearl_gpu_selftest_division(int device, const double* a, const double* b, lo
  * Runs on the calling thread's current device and on `stream` (NULL = legacy
  * default stream) and returns after the step has finished.
  *
- * All scratch comes from one array compiled into the library (about 32 MB,
+ * All scratch comes from one array compiled into the library (about 36 MB,
  * held by every GPU that loads the library until the process exits), so
  * nx*ny is limited to 262144 cells; larger domains return PEARL_ERR_TOO_LARGE.
  * The first call on each device looks up that array's device address; make
@@ -234,6 +236,41 @@ int pearl_gpu_selftest_division(int device, const double* a, const double* b, lo
 int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double* d_phi, double* d_carbon,
                               double* d_mu, pearl_scalars* scalars, double stop_time, pearl_step_info* out,
                               void* stream);
+
+/* ---- batched instances: a parameter sweep in one persistent launch ----
+ * n independent domains (each its own parameters and nx, ny) advance in one
+ * cooperative launch.  The grid is split into groups of `group_blocks`
+ * blocks, each group with its own grid barrier and reduction slots; the
+ * instances are assigned to groups longest-first, and a group runs its
+ * instances one after another.  Every instance follows exactly the path of a
+ * pearl_gpu_ctx (same kernels, same reduction order for the same group size),
+ * so it is main's loop (pearl_serial.cpp:2296-2306) run once per instance.
+ * No counterpart in the reference, which runs one case per process. */
+typedef struct pearl_gpu_batch pearl_gpu_batch;
+
+/* group_blocks <= 0 picks 4; pearl_gpu_batch_autotune can choose instead. */
+int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, const int* ny, int device,
+                           int group_blocks, pearl_gpu_batch** out);
+void pearl_gpu_batch_destroy(pearl_gpu_batch* batch);
+/* Host <-> device state of instance i, layouts as pearl_gpu_upload/download. */
+int pearl_gpu_batch_upload(pearl_gpu_batch* batch, int i, const double* phi_aos3, const double* carbon,
+                           const double* mu, const pearl_scalars* scalars);
+int pearl_gpu_batch_download(pearl_gpu_batch* batch, int i, double* phi_aos3, double* carbon, double* mu,
+                             pearl_scalars* scalars);
+/* Up to limits->max_steps accepted steps of every instance under the same
+ * limits, in one launch.  reports[i] and status[i] (pearl_status of instance
+ * i; an instance that fails stops, the others go on) may be NULL.  Returns
+ * PEARL_OK unless the launch itself failed. */
+int pearl_gpu_batch_run(pearl_gpu_batch* batch, const pearl_run_limits* limits, pearl_run_report* reports,
+                        int* status);
+/* Times `steps` one-step launches for each group size in {1,2,4,8,16} with
+ * and without TMA staging, restoring every instance's state after each
+ * trial, and keeps the fastest; the choice is written to the out pointers
+ * (may be NULL). */
+int pearl_gpu_batch_autotune(pearl_gpu_batch* batch, int steps, int* group_blocks, int* use_tma);
+int pearl_gpu_batch_stats(const pearl_gpu_batch* batch, long long* kernel_launches, int* grid_blocks,
+                          int* group_blocks, double* last_kernel_ms);
+const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* batch);
 
 #ifdef __cplusplus
 }
