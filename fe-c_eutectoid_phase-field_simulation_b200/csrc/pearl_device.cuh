@@ -113,7 +113,7 @@ struct Ctl {
 
 enum PhaseTag : int {
     kTagPropose = 0, kTagSetup, kTagApply, kTagUpdate, kTagTrueRes, kTagReset, kTagFinal, kTagEnergy,
-    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagSmooth, kTagInit, kTagCount
+    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagSmooth, kTagInit, kTagAdjoint, kTagCount
 };
 
 // ---------------------------------------------------------------- thermodynamics

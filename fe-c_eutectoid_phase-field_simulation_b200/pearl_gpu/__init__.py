@@ -117,11 +117,11 @@ EXPORTS = [
     "pearl_gpu_selftest_division", "pearl_gpu_advance_noalloc", "pearl_gpu_smooth_interface",
     "pearl_gpu_mixture_sums", "pearl_gpu_init_composition", "pearl_gpu_batch_create", "pearl_gpu_batch_destroy",
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
-    "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error",
+    "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient",
 ]
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
-          "mixture", "shift", "snapshot", "smooth", "init"]
+          "mixture", "shift", "snapshot", "smooth", "init", "adjoint"]
 
 _lib = None
 
@@ -168,6 +168,7 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_advance_noalloc.argtypes = [C.POINTER(PearlParams), C.c_int, C.c_int, V, V, V,
                                             C.POINTER(PearlScalars), D, C.POINTER(PearlStepInfo), V]
     IP = C.POINTER(C.c_int)
+    L.pearl_gpu_adjoint_gradient.argtypes = [V, C.c_longlong, C.c_int, DP, C.POINTER(PearlAdjointReport)]
     L.pearl_gpu_batch_create.argtypes = [C.c_int, C.POINTER(PearlParams), IP, IP, C.c_int, C.c_int, C.POINTER(V)]
     L.pearl_gpu_batch_destroy.argtypes = [V]
     L.pearl_gpu_batch_destroy.restype = None
@@ -192,6 +193,14 @@ def selftest_division(a: np.ndarray, b: np.ndarray, device: int = 0) -> int:
     if rc:
         raise PearlError(rc, STATUS.get(rc, str(rc)))
     return int(n.value)
+
+
+class PearlAdjointReport(C.Structure):
+    """pearl_adjoint_report: objective, gradient (mobility scale, sigma, D_gamma), counters, timings."""
+
+    _fields_ = [("objective", D), ("grad", D * 3), ("steps", C.c_longlong), ("cg_forward", C.c_longlong),
+                ("cg_adjoint", C.c_longlong), ("checkpoints", C.c_int), ("forward_ms", D), ("recompute_ms", D),
+                ("adjoint_ms", D)]
 
 
 class PearlError(RuntimeError):
@@ -340,6 +349,15 @@ class Context:
         v = C.c_int()
         self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
         return bool(v.value)
+
+    def adjoint_gradient(self, nsteps: int, checkpoint_every: int, target_alpha) -> PearlAdjointReport:
+        """Gradient of sum((phi_alpha - target)^2) after nsteps w.r.t. (mobility scale, sigma,
+        D_gamma); the context ends in the forward's final state."""
+        t = np.ascontiguousarray(target_alpha, dtype=np.float64)
+        assert t.shape == (self.ny, self.nx)
+        rep = PearlAdjointReport()
+        self._check(self.lib.pearl_gpu_adjoint_gradient(self.h, nsteps, checkpoint_every, _p(t), C.byref(rep)))
+        return rep
 
     def phase_times(self) -> dict:
         """{phase: (ms, count)} of the last launch."""

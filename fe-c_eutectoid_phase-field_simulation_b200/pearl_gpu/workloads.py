@@ -244,3 +244,34 @@ def sweep(n: int = 256, seed: int = 0) -> list[Workload]:
     """n sweep instances drawn from one seed (the batched-sweep workload)."""
     rng = np.random.default_rng(seed)
     return [sweep_instance(i, rng) for i in range(n)]
+
+
+ADJOINT_PARAMETERS = ("mobility", "sigma", "D_gamma")
+
+
+def perturb(params: dict, rel) -> dict:
+    """Parameters with the mobility scale (every 1/tau), sigma and D_gamma scaled by
+    (1 + rel[0]), (1 + rel[1]), (1 + rel[2])."""
+    p = dict(params)
+    p["tau"] = [t / (1.0 + rel[0]) for t in params["tau"]]
+    p["sigma"] = params["sigma"] * (1.0 + rel[1])
+    D = list(params["D"])
+    D[2] = D[2] * (1.0 + rel[2])
+    p["D"] = D
+    return p
+
+
+def adjoint_case(nx: int = 256, ny: int = 512, pairs: int = 4, steps: int = 1000, seed: int = 0,
+                 undercooling: float = 15.0, dt: float = 2e-12, front: float = 32.0) -> Workload:
+    """Adjoint workload: lamellar pairs (spacing nx/pairs, ferrite fraction 0.875), fixed dt
+    (dt_max = dt = 2e-12 s, small enough that no step is rejected at 15 K), `steps` steps.
+    meta['target_rel'] holds the seeded U(-5%, 5%) perturbation of (mobility, sigma,
+    D_gamma) whose forward run defines the target."""
+    rng = np.random.default_rng(seed)
+    dx = 2e-9
+    params = make_params(nx, ny, dx, undercooling=undercooling, dt=dt)
+    widths, thetas = jittered_pairs(nx, pairs, rng, 0.0, 0.875)
+    phi = lamellar_phi(nx, ny, widths, thetas, np.full(nx, front))
+    rel = [float(v) for v in rng.uniform(-0.05, 0.05, size=3)]
+    meta = dict(dt=dt, seed=seed, pairs=pairs, steps=steps, target_rel=rel)
+    return _finish(f"adjoint_{nx}x{ny}", nx, ny, params, phi, meta)

@@ -237,6 +237,33 @@ int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double
                               double* d_mu, pearl_scalars* scalars, double stop_time, pearl_step_info* out,
                               void* stream);
 
+/* ---- adjoint: gradient of a final-state misfit ----
+ * J = sum over cells of (phi_alpha - target_alpha)^2 after nsteps accepted
+ * steps from the context's current state, and dJ/dtheta for
+ * theta = (M, sigma, D_gamma): M is a common scale on every interface
+ * mobility 1/tau (the forward runs at M = 1), sigma the interface energy,
+ * D_gamma the austenite diffusivity.  Reverse mode: the forward stores a
+ * checkpoint every `checkpoint_every` steps and the accepted dt of every
+ * step; the reverse sweep recomputes each segment from its checkpoint with
+ * that dt sequence (recording every state and diffusion solution), then runs
+ * the segment's adjoint steps backwards on the device.  The step is
+ * differentiated as computed (propose_phi, pearl_serial.cpp:961-1002, with
+ * the simplex projection on its active set; implicit_diffusion, :1010-1093,
+ * with the linear system taken as solved exactly); acceptance decisions are
+ * held fixed.  On success the context holds the forward's final state; on
+ * error, its initial state.  No counterpart in the reference. */
+typedef struct pearl_adjoint_report {
+    double objective;
+    double grad[3]; /* dJ/dM, dJ/dsigma, dJ/dD_gamma */
+    long long steps, cg_forward, cg_adjoint;
+    int checkpoints;
+    double forward_ms, recompute_ms, adjoint_ms; /* device time of the three sweeps */
+} pearl_adjoint_report;
+
+/* target_alpha[y*nx+x] on the host. */
+int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, int checkpoint_every,
+                               const double* target_alpha, pearl_adjoint_report* out);
+
 /* ---- batched instances: a parameter sweep in one persistent launch ----
  * n independent domains (each its own parameters and nx, ny) advance in one
  * cooperative launch.  The grid is split into groups of `group_blocks`

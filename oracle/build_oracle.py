@@ -48,10 +48,11 @@ def _stale(out: Path, *inputs: Path) -> bool:
 
 def build_port(force: bool = False) -> Path:
     src = HERE / "pearl_oracle.c"
+    adj = HERE / "pearl_adjoint.c"
     hdr = HERE / "pearl_oracle.h"
-    if force or _stale(ORACLE_SO, src, hdr):
+    if force or _stale(ORACLE_SO, src, adj, hdr):
         _run(["gcc", "-std=c99", "-O3", "-ffp-contract=off", "-fPIC", "-shared", "-Wall", "-Wextra", "-Wno-maybe-uninitialized",
-              str(src), "-o", str(ORACLE_SO), "-lm"])
+              str(src), str(adj), "-o", str(ORACLE_SO), "-lm"])
     return ORACLE_SO
 
 

@@ -254,10 +254,11 @@ static double dot(const double* a, const double* b, size_t n) {
     return s;
 }
 
-/* implicit_diffusion, pearl_serial.cpp:1010-1094 */
-int po_implicit_diffusion(const po_params* p, int nx, int ny, const double* carbon_old, const double* mu_old,
-                          const double* trial_phi, double* trial_carbon, double* trial_mu, double dt,
-                          po_diffusion_info* info) {
+/* implicit_diffusion, pearl_serial.cpp:1010-1094.  u_out (may be NULL) receives
+ * the converged solution u = mu - mu_reference of the linear system. */
+int po_implicit_diffusion_u(const po_params* p, int nx, int ny, const double* carbon_old, const double* mu_old,
+                            const double* trial_phi, double* trial_carbon, double* trial_mu, double dt,
+                            po_diffusion_info* info, double* u_out) {
     const size_t n = (size_t)nx * (size_t)ny;
     const double mu_r = p->mu_reference;
     double* mem = (double*)malloc(sizeof(double) * n * 10);
@@ -352,8 +353,15 @@ int po_implicit_diffusion(const po_params* p, int nx, int ny, const double* carb
     inf.closure = closure;
     inf.ok = closure <= p->closure_tol;
     *info = inf;
+    if (u_out) memcpy(u_out, u, sizeof(double) * n);
     free(mem);
     return PO_OK;
+}
+
+int po_implicit_diffusion(const po_params* p, int nx, int ny, const double* carbon_old, const double* mu_old,
+                          const double* trial_phi, double* trial_carbon, double* trial_mu, double dt,
+                          po_diffusion_info* info) {
+    return po_implicit_diffusion_u(p, nx, ny, carbon_old, mu_old, trial_phi, trial_carbon, trial_mu, dt, info, NULL);
 }
 
 /* valid_state, pearl_serial.cpp:1096-1116 */

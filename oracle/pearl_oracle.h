@@ -103,6 +103,10 @@ int po_propose_phi(const po_params* p, int nx, int ny, const double* phi_old, co
 int po_implicit_diffusion(const po_params* p, int nx, int ny, const double* carbon_old, const double* mu_old,
                           const double* trial_phi, double* trial_carbon, double* trial_mu, double dt,
                           po_diffusion_info* info);
+/* implicit_diffusion that also returns the converged u = mu - mu_reference (u_out may be NULL). */
+int po_implicit_diffusion_u(const po_params* p, int nx, int ny, const double* carbon_old, const double* mu_old,
+                            const double* trial_phi, double* trial_carbon, double* trial_mu, double dt,
+                            po_diffusion_info* info, double* u_out);
 int po_valid_state(const po_params* p, int nx, int ny, const double* phi, const double* carbon,
                    const double* mu);
 /* One accepted step.  Fields are updated in place on success.  *why receives the
@@ -136,6 +140,28 @@ typedef struct po_smooth_report {
 } po_smooth_report;
 int po_smooth_interface_only(const po_params* p, int nx, int ny, double* phi, int max_steps, int min_steps,
                              double energy_rtol, double max_phase_change, po_smooth_report* report);
+
+/* ---- adjoint (no reference counterpart: the reference has no gradient) ----
+ * Reverse-mode gradient of J = sum over cells of (phi_alpha - target)^2 after
+ * nsteps accepted steps, with respect to theta = (mobility scale M, sigma,
+ * D_gamma) at the given parameters.  M multiplies every interface mobility
+ * 1/tau (the forward runs at M = 1).  The discrete step is differentiated as
+ * computed: propose_phi (forces, local tau, simplex projection on its active
+ * set) and implicit_diffusion with its linear system treated as solved
+ * exactly.  The forward keeps a checkpoint every checkpoint_every steps; the
+ * reverse sweep recomputes each segment from its checkpoint with the recorded
+ * accepted dt sequence.  On return the fields hold the forward's final state. */
+typedef struct po_adjoint_report {
+    double objective;
+    double grad[3]; /* dJ/dM, dJ/dsigma, dJ/dD_gamma */
+    long long steps, cg_forward, cg_adjoint;
+    int checkpoints;
+} po_adjoint_report;
+int po_adjoint_gradient(const po_params* p, int nx, int ny, double* phi, double* carbon, double* mu, po_scalars* s,
+                        int nsteps, int checkpoint_every, const double* target_alpha, po_adjoint_report* out);
+/* J only: nsteps accepted steps of the forward, then the misfit (fields updated in place). */
+int po_adjoint_objective(const po_params* p, int nx, int ny, double* phi, double* carbon, double* mu,
+                         po_scalars* s, int nsteps, const double* target_alpha, double* objective);
 
 #ifdef __cplusplus
 }

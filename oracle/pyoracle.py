@@ -57,6 +57,11 @@ class PoDiffusionInfo(C.Structure):
     _fields_ = [("ok", C.c_int), ("it", C.c_int), ("residual", D), ("closure", D)]
 
 
+class PoAdjointReport(C.Structure):
+    _fields_ = [("objective", D), ("grad", D * 3), ("steps", C.c_longlong), ("cg_forward", C.c_longlong),
+                ("cg_adjoint", C.c_longlong), ("checkpoints", C.c_int)]
+
+
 class PoDiag(C.Structure):
     _fields_ = [(n, D) for n in ("c_min", "c_max", "mu_min", "mu_max", "phi_sum_error", "mass", "ledger", "energy")]
 
@@ -139,6 +144,10 @@ class Port(_Lib):
         L.po_close_mu.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP]
         L.po_psi.argtypes = [C.POINTER(PoParams), C.c_int, D]
         L.po_psi.restype = D
+        L.po_adjoint_gradient.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP, C.POINTER(PoScalars),
+                                          C.c_int, C.c_int, DP, C.POINTER(PoAdjointReport)]
+        L.po_adjoint_objective.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP,
+                                           C.POINTER(PoScalars), C.c_int, DP, DP]
 
     def psi(self, params, phase: int, mu: float) -> float:
         return self.lib.po_psi(C.byref(_params(params)), phase, mu)
@@ -213,6 +222,25 @@ class Port(_Lib):
         mu = np.empty_like(carbon)
         rc = self.lib.po_close_mu(C.byref(_params(params)), nx, ny, _p(phi), _p(carbon), _p(mu))
         return rc, mu
+
+
+    def adjoint_gradient(self, params, phi, carbon, mu, scalars, nsteps, checkpoint_every, target_alpha):
+        """Reverse-mode gradient of sum((phi_alpha - target)^2) after nsteps, w.r.t.
+        (mobility scale, sigma, D_gamma).  Fields advance in place.  Returns (rc, report)."""
+        ny, nx = mu.shape
+        rep = PoAdjointReport()
+        t = np.ascontiguousarray(target_alpha, dtype=np.float64)
+        rc = self.lib.po_adjoint_gradient(C.byref(_params(params)), nx, ny, _p(phi), _p(carbon), _p(mu),
+                                          C.byref(scalars), nsteps, checkpoint_every, _p(t), C.byref(rep))
+        return rc, rep
+
+    def adjoint_objective(self, params, phi, carbon, mu, scalars, nsteps, target_alpha):
+        ny, nx = mu.shape
+        J = D()
+        t = np.ascontiguousarray(target_alpha, dtype=np.float64)
+        rc = self.lib.po_adjoint_objective(C.byref(_params(params)), nx, ny, _p(phi), _p(carbon), _p(mu),
+                                           C.byref(scalars), nsteps, _p(t), C.byref(J))
+        return rc, J.value
 
 
 class Reference(_Lib):
