@@ -59,9 +59,11 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="bound of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=60.0, help="bound of the reference arm's timed work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["plain_large", "sweep"], default="plain_large",
+    ap.add_argument("--workload", choices=["plain_large", "sweep", "adjoint"], default="plain_large",
                     help="plain_large (default): one 2048x4096 domain; sweep: 256 small independent "
-                         "instances in one batched persistent launch")
+                         "instances in one batched persistent launch; adjoint: gradient of a 256x512, "
+                         "1000-step run (--steps sets the step count of that run)")
+    ap.add_argument("--checkpoint-every", type=int, default=50, help="adjoint: steps per checkpoint segment")
     ap.add_argument("--instances", type=int, default=256, help="sweep: number of instances")
     ap.add_argument("--group-blocks", type=int, default=0, help="sweep: blocks per instance group (0 = autotune)")
     return ap.parse_args(argv)
@@ -478,6 +480,130 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
     b.close()
 
 
+def adjoint_arm(args, rank: int, world: int, dist) -> None:
+    """Gradient of J = sum (phi_alpha - target)^2 after K fixed-dt steps of a 256x512
+    domain (4 lamellar pairs of spacing 64, ferrite fraction 0.875, T_E-15 K, dt 2e-12 s)
+    w.r.t. (mobility scale, sigma, D_gamma); the target comes from a forward run with
+    the three parameters perturbed by seeded U(-5%, 5%).  One timed step = one whole
+    gradient (forward with checkpoints, recomputation, adjoint sweep).  Metric:
+    gradient cell-steps/s = cells * K / gradient time."""
+    import numpy as np
+    import torch
+
+    import pearl_gpu
+    from pearl_gpu import workloads as W
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    K = args.steps
+    w = W.adjoint_case(steps=K, seed=rank)
+    every = args.checkpoint_every
+
+    def ctx_for(params):
+        c = pearl_gpu.Context(params, w.nx, w.ny, device=local)
+        c.upload(w.phi, w.carbon, w.mu, w.scalars)
+        return c
+
+    with ctx_for(W.perturb(w.params, w.meta["target_rel"])) as c:
+        c.run(K)
+        target = np.ascontiguousarray(c.download()[0][..., 0])
+    phi_h = torch.from_numpy(w.phi).pin_memory().numpy()
+    c_h = torch.from_numpy(w.carbon).pin_memory().numpy()
+    mu_h = torch.from_numpy(w.mu).pin_memory().numpy()
+    ctx = pearl_gpu.Context(w.params, w.nx, w.ny, device=local)
+    for _ in range(max(args.warmup, 1)):
+        ctx.upload(phi_h, c_h, mu_h, w.scalars)
+        ctx.adjoint_gradient(K, every, target)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    l0 = ctx.stats()["launches"]
+    clocks.start()
+    t0 = time.perf_counter()
+    ctx.upload(phi_h, c_h, mu_h, w.scalars)
+    rep = ctx.adjoint_gradient(K, every, target)
+    out = ctx.download()
+    barrier()
+    wall = time.perf_counter() - t0
+    clock_info = clocks.stop()
+    launches = ctx.stats()["launches"] - l0
+    dev_ms = rep.forward_ms + rep.recompute_ms + rep.adjoint_ms
+    cell_steps = float(w.cells * K)
+    value, t_max = replica_throughput(dist, cell_steps, dev_ms / 1e3, "cuda")
+    e2e_value, _ = replica_throughput(dist, cell_steps, wall, "cuda")
+    # central differences of the device forward (h = 1e-6 relative)
+    h = 1e-6
+    base = [1.0, w.params["sigma"], w.params["D"][2]]
+    fd_err = {}
+    for k in range(3):
+        J = []
+        for sign in (1, -1):
+            rel = [0.0, 0.0, 0.0]
+            rel[k] = sign * h
+            with ctx_for(W.perturb(w.params, rel)) as c:
+                c.run(K)
+                J.append(float(((c.download()[0][..., 0] - target) ** 2).sum()))
+        fd = (J[0] - J[1]) / (2 * h * base[k])
+        fd_err[W.ADJOINT_PARAMETERS[k]] = abs(rep.grad[k] - fd) / abs(fd)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the CPU reference gradient (oracle/pearl_adjoint.c, one core) on a bounded
+        # prefix of the same run, and the device gradient of that prefix beside it
+        from oracle import pyoracle
+
+        port = pyoracle.port()
+        kp = min(K, 100)
+        phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+        s = pyoracle.scalars_from(w.scalars)
+        tc = time.perf_counter()
+        rc, orep = port.adjoint_gradient(w.params, phi, c, mu, s, kp, min(every, kp), target)
+        secs = time.perf_counter() - tc
+        if rc:
+            raise RuntimeError("CPU reference gradient failed")
+        ctx.upload(phi_h, c_h, mu_h, w.scalars)
+        prep = ctx.adjoint_gradient(kp, min(every, kp), target)
+        cpu = {"value": w.cells * kp / secs, "unit": "gradient cell-steps/s", "cores": 1, "kind": "port",
+               "sample": f"CPU reference gradient of the first {kp} steps ({secs:.1f} s, single thread)",
+               "gpu_vs_cpu_gradient_rel_err": {W.ADJOINT_PARAMETERS[k]: abs(prep.grad[k] - orep.grad[k])
+                                               / abs(orep.grad[k]) for k in range(3)},
+               "cpu": _cpu_model()}
+    ctx.close()
+    if rank == 0:
+        per_step = 2 * (80.0 + 64.0 * rep.cg_forward / K) + 48.0 + 160.0 + 64.0 * rep.cg_adjoint / K
+        algo = per_step * cell_steps
+        peak, peak_kind = measured_peak()
+        line = {
+            "metric": "gradient cell-steps/s", "value": value, "unit": "gradient cell-steps/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": t_max / K * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"adjoint: {w.nx}x{w.ny}, 4 pairs spacing 64, f_alpha 0.875, T_E-15K, "
+                                   f"dt 2e-12 s fixed, {K} steps, checkpoint every {every}",
+                       "parameters": list(W.ADJOINT_PARAMETERS), "target_rel": w.meta["target_rel"],
+                       "objective": rep.objective, "gradient": list(rep.grad),
+                       "fd_rel_err": fd_err, "cg_forward": rep.cg_forward, "cg_adjoint": rep.cg_adjoint,
+                       "forward_ms": rep.forward_ms, "recompute_ms": rep.recompute_ms,
+                       "adjoint_ms": rep.adjoint_ms, "l2": "state 5 MB, tape 300 MB per segment",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": algo / (dev_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / (dev_ms / 1e3) / 1e9 / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} HBM copy bandwidth",
+                         "kernel": "pearl_kernel (forward, recompute with tape) + pearl_adjoint_kernel",
+                         "bytes_per_cell_step": "2*(80+64*n_CG) + 48 tape + 160 adjoint + 64*n_CG_adjoint"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "gradient cell-steps/s", "h2d_bytes_per_step": 48 * w.cells / K,
+                    "d2h_bytes_per_step": 40 * w.cells / K,
+                    "step": "upload state and target, whole gradient, download final state"},
+            "clocks": clock_info,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -499,6 +625,8 @@ def main(argv=None) -> int:
             reference_arm(args, rank, world)
         elif args.workload == "sweep":
             sweep_arm(args, rank, world, dist)
+        elif args.workload == "adjoint":
+            adjoint_arm(args, rank, world, dist)
         else:
             gpu_arm(args, rank, world, dist)
     finally:

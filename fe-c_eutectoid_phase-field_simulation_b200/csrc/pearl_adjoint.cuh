@@ -137,46 +137,50 @@ __device__ bool adj_step(const Dom& a, Red& red, const AdjArgs& g, const double*
     const AdjBufs& J = g.J;
     const size_t pe = (size_t)P.pitch * P.ny;
     const double* u = s1 + 5 * pe;
-    // P1: trial mixture and u^ = mu'^ + chi c'^
-    double ub2 = 0;
+    // SET-UP (one pass): trial mixture, u^ = mu'^ + chi c'^, and the Jacobi-PCG
+    // start for A lambda = u^ warm-started from the previous reverse step's
+    // lambda (the adjoint carbon of consecutive steps differs little).  K at
+    // the neighbours is recomputed from their trial phi, so no pass is needed
+    // between writing K and reading it.
+    double ub2 = 0, rz = 0, rr = 0;
     FOR_CELLS(P) {
         const Cell c = cell_at(P, idx_);
         double q[3];
         load3p(s1, pe, c.i, q);
-        double chi, cint, K;
-        mixture(P, q[0], q[1], q[2], chi, cint, K);
-        J.chi[c.i] = chi;
-        J.K[c.i] = K;
+        double chi, cint, k;
+        mixture(P, q[0], q[1], q[2], chi, cint, k);
         const double ub = J.bmu[c.i] + chi * J.bc[c.i];
-        J.ub[c.i] = ub;
-        ub2 += ub * ub;
-    }
-    double v1[1] = {ub2};
-    if (!red.reduce<1>(v1, kSum, kTagAdjoint)) return false;
-    ub2 = v1[0];
-    // P2: Jacobi-PCG set-up for A lambda = u^ from lambda = 0
-    double rz = 0;
-    FOR_CELLS(P) {
-        const Cell c = cell_at(P, idx_);
-        const double k = J.K[c.i];
-        double ws = 0;
+        const double l0 = J.lam[c.i];
+        double ws = 0, al = 0;
 #pragma unroll
         for (int d = 0; d < 4; ++d)
-            if (c.has[d]) ws += adj_face(P, k, J.K[c.n[d]], d);
-        const double diag = J.chi[c.i] + dt * ws;
-        const double r = J.ub[c.i];
+            if (c.has[d]) {
+                double qn[3];
+                load3p(s1, pe, c.n[d], qn);
+                const double kn = qn[0] * P.D[0] * P.chi_p[0] + qn[1] * P.D[1] * P.chi_p[1] + qn[2] * P.D[2] * P.chi_p[2];
+                const double w = adj_face(P, k, kn, d);
+                ws += w;
+                al += w * (l0 - J.lam[c.n[d]]);
+            }
+        const double diag = chi + dt * ws;
+        const double r = ub - (chi * l0 + dt * al);
         const double z = r / diag;
+        J.chi[c.i] = chi;
+        J.K[c.i] = k;
         J.diag[c.i] = diag;
-        J.lam[c.i] = 0;
         J.r[c.i] = r;
         J.z[c.i] = z;
+        ub2 += ub * ub;
         rz += r * z;
+        rr += r * r;
     }
-    v1[0] = rz;
-    if (!red.reduce<1>(v1, kSum, kTagAdjoint)) return false;
-    rz = v1[0];
-    double rr = ub2;
+    double v3s[3] = {ub2, rz, rr};
+    if (!red.reduce<3>(v3s, OPS3(kSum, kSum, kSum), kTagAdjoint)) return false;
+    ub2 = v3s[0];
+    rz = v3s[1];
+    rr = v3s[2];
     const double tol = P.cg_rtol * sqrt(ub2);
+    double v1[1];
     int it = 0, pb = 0;
     double beta = 0;
     bool first = true;

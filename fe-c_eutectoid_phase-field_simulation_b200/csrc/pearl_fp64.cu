@@ -2612,6 +2612,11 @@ extern "C" int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, 
             a.mode = kModeRun;
             a.L = pearl_run_limits{len, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
             a.dt_log = dts + k0;
+            if (seg == nseg - 1) {
+                // the reverse sweep starts here: tape this segment now instead of recomputing it
+                a.tape = tape;
+                a.tape_slot = 6 * pe;
+            }
             int rc = launch(ctx, a);
             if (rc) return rc;
             if (ctx->h_ctl->steps != len) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "forward stopped early");
@@ -2635,21 +2640,24 @@ extern "C" int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, 
         double recompute_ms = 0;
         for (long long seg = nseg - 1; seg >= 0; --seg) {
             const long long k0 = seg * K, len = std::min(K, nsteps - k0);
-            PG_CUDA(ctx, cudaMemcpyAsync(state(0), ckpt + (size_t)seg * 5 * pe, 5 * pe * sizeof(double),
-                                         cudaMemcpyDeviceToDevice, ctx->stream));
-            ctx->h_ctl->cur = 0;
-            ctx->h_ctl->S = seg_scalars[seg];
-            ctx->h_ctl->energy_valid = 0;
-            KArgs a{};
-            a.mode = kModeRun;
-            a.L = pearl_run_limits{len, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
-            a.forced_dt = dts + k0;
-            a.tape = tape;
-            a.tape_slot = 6 * pe;
-            rc = launch(ctx, a);
-            if (rc) return rc;
-            recompute_ms += ctx->last_ms;
-            if (ctx->h_ctl->steps != len) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "recomputation stopped early");
+            if (seg < nseg - 1) {
+                PG_CUDA(ctx, cudaMemcpyAsync(state(0), ckpt + (size_t)seg * 5 * pe, 5 * pe * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, ctx->stream));
+                ctx->h_ctl->cur = 0;
+                ctx->h_ctl->S = seg_scalars[seg];
+                ctx->h_ctl->energy_valid = 0;
+                KArgs a{};
+                a.mode = kModeRun;
+                a.L = pearl_run_limits{len, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
+                a.forced_dt = dts + k0;
+                a.tape = tape;
+                a.tape_slot = 6 * pe;
+                rc = launch(ctx, a);
+                if (rc) return rc;
+                recompute_ms += ctx->last_ms;
+                if (ctx->h_ctl->steps != len)
+                    return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "recomputation stopped early");
+            }
             g.mode = 1;
             g.ckpt = ckpt + (size_t)seg * 5 * pe;
             g.tape = tape;

@@ -244,9 +244,11 @@ int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double
  * mobility 1/tau (the forward runs at M = 1), sigma the interface energy,
  * D_gamma the austenite diffusivity.  Reverse mode: the forward stores a
  * checkpoint every `checkpoint_every` steps and the accepted dt of every
- * step; the reverse sweep recomputes each segment from its checkpoint with
- * that dt sequence (recording every state and diffusion solution), then runs
- * the segment's adjoint steps backwards on the device.  The step is
+ * step, and records the last segment's states and diffusion solutions on a
+ * tape; the reverse sweep recomputes every other segment from its
+ * checkpoint with that dt sequence (recording it on the tape), then runs the
+ * segment's adjoint steps backwards on the device, each adjoint linear solve
+ * warm-started from the previous one.  The step is
  * differentiated as computed (propose_phi, pearl_serial.cpp:961-1002, with
  * the simplex projection on its active set; implicit_diffusion, :1010-1093,
  * with the linear system taken as solved exactly); acceptance decisions are

@@ -101,3 +101,48 @@ def test_adjoint_checkpoint_interval_and_repeat(gpu_lib):
     for k in range(3):
         assert reps[1].grad[k] == pytest.approx(reps[0].grad[k], rel=1e-12)
         assert again.grad[k] == reps[0].grad[k]
+
+
+def test_autograd_function_wrapper(gpu_lib):
+    """The C-ABI gradient as a torch.autograd.Function (test harness only): theta are
+    multipliers of (mobility, sigma, D_gamma); backward returns dJ/dtheta."""
+    import torch
+
+    from pearl_gpu import workloads as W
+
+    steps = 40
+    w = _case(nx=64, ny=64, steps=steps)
+    target = _target(w, steps)
+    base = [1.0, w.params["sigma"], w.params["D"][2]]
+
+    class Misfit(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, theta):
+            rel = [float(t) - 1.0 for t in theta.detach().cpu()]
+            params = W.perturb(w.params, rel)
+            with _ctx(w, params) as ctx:
+                rep = ctx.adjoint_gradient(steps, 10, target)
+            th = [float(t) for t in theta.detach().cpu()]
+            # the context's own mobility scale M multiplies theta_0; sigma and D_gamma scale linearly
+            g = [rep.grad[0] / th[0], rep.grad[1] * base[1], rep.grad[2] * base[2]]
+            fctx.save_for_backward(torch.tensor(g, dtype=torch.float64))
+            return torch.tensor(rep.objective, dtype=torch.float64)
+
+        @staticmethod
+        def backward(fctx, gout):
+            (g,) = fctx.saved_tensors
+            return gout * g
+
+    theta = torch.tensor([1.02, 0.97, 1.01], dtype=torch.float64, requires_grad=True)
+    J = Misfit.apply(theta)
+    J.backward()
+    h = 1e-6
+    for k in range(3):
+        Js = []
+        for sign in (1, -1):
+            t = theta.detach().clone()
+            t[k] += sign * h
+            rel = [float(x) - 1.0 for x in t]
+            Js.append(_objective(w, W.perturb(w.params, rel), steps, target))
+        fd = (Js[0] - Js[1]) / (2 * h)
+        assert float(theta.grad[k]) == pytest.approx(fd, rel=RTOL)
