@@ -64,6 +64,8 @@ def parse_args(argv=None):
                          "instances in one batched persistent launch; adjoint: gradient of a 256x512, "
                          "1000-step run (--steps sets the step count of that run)")
     ap.add_argument("--checkpoint-every", type=int, default=50, help="adjoint: steps per checkpoint segment")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="fp64 (default): the reference's arithmetic; mixed: FP32 propose forces")
     ap.add_argument("--instances", type=int, default=256, help="sweep: number of instances")
     ap.add_argument("--group-blocks", type=int, default=0, help="sweep: blocks per instance group (0 = autotune)")
     return ap.parse_args(argv)
@@ -84,6 +86,7 @@ def config_dict(w, args) -> dict:
         "l2": "inputs larger than L2 (state 40 B/cell = %.0f MB)" % (40 * w.cells / 1e6),
         "parallelism": f"replicas x{args.gpus}",
         "bytes_per_cell_update": "80 + 64*n_CG",
+        "precision": args.precision,
     }
 
 
@@ -279,6 +282,7 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
     stream = torch.cuda.current_stream()
     w = workload(args.nx, args.ny, seed=rank)
     ctx = pearl_gpu.Context(w.params, w.nx, w.ny, device=local, stream=stream.cuda_stream)
+    ctx.set_precision(args.precision)
     # pinned host buffers for the end-to-end leg
     phi_h = torch.from_numpy(w.phi).pin_memory().numpy()
     c_h = torch.from_numpy(w.carbon).pin_memory().numpy()
@@ -364,8 +368,8 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(w, args),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic", "config": config_dict(w, args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",

@@ -45,6 +45,14 @@ struct DevParams {
     // RN(1/b) of every constant divisor b, for div_by
     double r_Vm, r_dx, r_dy, r_dx2, r_dy2, r_3, r_two_A[3];
     int exact_div;  // 1 when every constant divisor and its reciprocal are normal numbers
+    // Mixed precision (PROPOSE forces in FP32).  psi_b(mu) - psi_g(mu) is
+    // expanded about mu_ref in delta = mu - mu_ref, which is formed in FP64:
+    // m_pa[b] + delta*(m_pb[b] + delta*m_pc[b]), so FP32 never subtracts two
+    // large free energies.
+    int mixed;
+    float m_obs, m_tr, m_kx, m_ky, m_rVm;  // obs, tr, 2 eps sigma / dx^2, / dy^2, 1/Vm
+    float m_pa[2], m_pb[2], m_pc[2];
+    float m_tau[3], m_tau_min;
 };
 
 // a/b, correctly rounded, for a divisor b whose reciprocal rb = RN(1/b) was

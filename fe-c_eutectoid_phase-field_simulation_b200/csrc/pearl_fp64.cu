@@ -27,6 +27,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -543,6 +544,66 @@ __device__ __forceinline__ Proposal propose_cell(const DevParams& P, const Src& 
     return o;
 }
 
+// propose_phi with the forces, local tau and increment in FP32 (mixed
+// precision); the state stays FP64: z = q - (double)increment, and the
+// projection and max |dphi| are FP64 as in propose_cell.
+template <class Src>
+__device__ __forceinline__ Proposal propose_cell_mixed(const DevParams& P, const Src& src, int k, double dt,
+                                                       bool south, bool north) {
+    const double q0 = src.v(0, k, kC), q1 = src.v(1, k, kC), q2 = src.v(2, k, kC);
+    const float del = (float)(src.v(3, k, kC) - P.mu_ref);
+    const float q[3] = {(float)q0, (float)q1, (float)q2};
+    float dps[2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) dps[b] = __fmaf_rn(del, __fmaf_rn(del, P.m_pc[b], P.m_pb[b]), P.m_pa[b]);
+    const float dtr[3] = {2.0f * q[1] * q[2], 2.0f * q[0] * q[2], 2.0f * q[0] * q[1]};
+    float f[3];
+#pragma unroll
+    for (int aa = 0; aa < 3; ++aa) {
+        const float qa1 = q[(aa + 1) % 3], qa2 = q[(aa + 2) % 3];
+        f[aa] = P.m_obs * (qa1 + qa2) + P.m_tr * qa1 * qa2;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float dh = dtr[aa] + (b == aa ? 6.0f * q[b] * (1.0f - q[b]) : 0.0f);
+            f[aa] += dps[b] * dh * P.m_rVm;
+        }
+    }
+#pragma unroll
+    for (int dir = 0; dir < 4; ++dir) {
+        if ((dir == 2 && !south) || (dir == 3 && !north)) continue;
+        const int d = dir == 0 ? kW : dir == 1 ? kE : dir == 2 ? kS : kN;
+        const float n[3] = {(float)src.v(0, k, d), (float)src.v(1, k, d), (float)src.v(2, k, d)};
+        const float kk = dir < 2 ? P.m_kx : P.m_ky;
+#pragma unroll
+        for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+            for (int b = aa + 1; b < 3; ++b) {
+                const float w = kk * __fmaf_rn(q[aa], n[b], -n[aa] * q[b]);
+                f[aa] = __fmaf_rn(w, n[b], f[aa]);
+                f[b] = __fmaf_rn(-w, n[aa], f[b]);
+            }
+    }
+    const float mean = (f[0] + f[1] + f[2]) * (1.0f / 3.0f);
+    const float w0 = q[0] * q[1], w1 = q[0] * q[2], w2 = q[1] * q[2], ws = w0 + w1 + w2;
+    const float tau = ws > 1e-30f ? (w0 * P.m_tau[0] + w1 * P.m_tau[1] + w2 * P.m_tau[2]) / ws : P.m_tau_min;
+    const float scale = (float)(dt / ((double)tau * P.eps));
+    Proposal o;
+    o.z0 = q0 - (double)(scale * (f[0] - mean));
+    o.z1 = q1 - (double)(scale * (f[1] - mean));
+    o.z2 = q2 - (double)(scale * (f[2] - mean));
+    o.simplex_bad = false;
+    if (!(isfinite(o.z0) && isfinite(o.z1) && isfinite(o.z2))) {
+        o.change = INFINITY;
+        o.z0 = q0;
+        o.z1 = q1;
+        o.z2 = q2;
+    } else {
+        o.simplex_bad = !project_simplex(P, o.z0, o.z1, o.z2);
+        o.change = fmax(fmax(fabs(o.z0 - q0), fabs(o.z1 - q1)), fabs(o.z2 - q2));
+    }
+    return o;
+}
+
 // PROPOSE: propose_phi from state `cur` into state `1-cur`, then the mixture of
 // the trial phi (K, chi, icpt); in phase_only mode also the reconstructed
 // trial carbon and the copied trial mu (pearl_serial.cpp:1134-1136).
@@ -556,13 +617,16 @@ __device__ bool phase_propose(const Dom& a, Red& red, int cur, double dt, double
     const int maps[4] = {kMapState + 5 * cur, kMapState + 5 * cur + 1, kMapState + 5 * cur + 2,
                          kMapState + 5 * cur + 4};
     const double* const planes[4] = {B.phi[cur][0], B.phi[cur][1], B.phi[cur][2], B.mu[cur]};
-    const bool ok = sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, [&](const auto& src, const Pair& c) {
+    // the FP64 and the mixed-precision proposal are separate sweeps, so each
+    // loop is register-allocated on its own
+    const auto body = [&](auto mixed_tag, const auto& src, const Pair& c) {
 #pragma unroll 1
         for (int k = 0; k < 2; ++k) {
             if (k == 1 && !c.v1) break;
             const int y = c.y0 + k;
             const size_t i = k ? c.i1 : c.i0;
-            const Proposal o = propose_cell(P, src, k, dt, y > 0, y < P.ny - 1);
+            const Proposal o = decltype(mixed_tag)::value ? propose_cell_mixed(P, src, k, dt, y > 0, y < P.ny - 1)
+                                                          : propose_cell(P, src, k, dt, y > 0, y < P.ny - 1);
             if (o.change == INFINITY)
                 vchange = INFINITY;
             else
@@ -582,7 +646,12 @@ __device__ bool phase_propose(const Dom& a, Red& red, int cur, double dt, double
                 B.mu[cur ^ 1][i] = mu;
             }
         }
-    });
+    };
+    const bool ok =
+        P.mixed ? sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u,
+                           [&](const auto& src, const Pair& c) { body(std::true_type{}, src, c); })
+                : sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u,
+                           [&](const auto& src, const Pair& c) { body(std::false_type{}, src, c); });
     if (!ok) return false;
     double v[3] = {vchange, vmix, vsimp};
     if (!red.reduce<3>(v, OPS3(kMax, kMax, kMax), kTagPropose)) return false;
@@ -1902,6 +1971,20 @@ void fill_dev_params(pearl_gpu_ctx* ctx) {
     }
     P.tau_min = tmin;
     P.mu_ref = p->mu_reference;
+    // mixed-precision constants (P.mixed itself is set by pearl_gpu_set_precision)
+    P.m_obs = (float)P.obs;
+    P.m_tr = (float)P.tr;
+    P.m_kx = (float)(P.two_eps_sigma / P.dx2);
+    P.m_ky = (float)(P.two_eps_sigma / P.dy2);
+    P.m_rVm = (float)(1.0 / p->Vm);
+    for (int b = 0; b < 2; ++b) {
+        const double mr = p->mu_reference;
+        P.m_pa[b] = (float)(host_psi(p, b, mr) - host_psi(p, 2, mr));
+        P.m_pb[b] = (float)(-(mr - p->B[b]) / (2.0 * p->A[b]) + (mr - p->B[2]) / (2.0 * p->A[2]));
+        P.m_pc[b] = (float)(-0.25 / p->A[b] + 0.25 / p->A[2]);
+    }
+    for (int i = 0; i < 3; ++i) P.m_tau[i] = (float)p->tau[i];
+    P.m_tau_min = (float)tmin;
     P.psi_t[0] = host_psi(p, 0, p->mu_reference) - host_psi(p, 2, p->mu_reference);
     P.psi_t[1] = host_psi(p, 1, p->mu_reference) - host_psi(p, 2, p->mu_reference);
     P.psi_t[2] = 0;
@@ -2232,6 +2315,13 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
 int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream) {
     if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
     ctx->stream = (cudaStream_t)stream;
+    return PEARL_OK;
+}
+
+int pearl_gpu_set_precision(pearl_gpu_ctx* ctx, int precision) {
+    if (!ctx || (precision != PEARL_PRECISION_FP64 && precision != PEARL_PRECISION_MIXED))
+        return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid precision");
+    ctx->P.mixed = precision == PEARL_PRECISION_MIXED;
     return PEARL_OK;
 }
 
@@ -2997,6 +3087,15 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
     if (group_blocks) *group_blocks = best_gb;
     if (use_tma) *use_tma = best_tma ? 1 : 0;
     return rc;
+}
+
+int pearl_gpu_batch_set_precision(pearl_gpu_batch* b, int precision) {
+    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
+    for (auto* c : b->inst) {
+        const int rc = pearl_gpu_set_precision(c, precision);
+        if (rc) return bfail(b, rc, "invalid precision");
+    }
+    return batch_configure(b, b->group_blocks, b->use_tma);
 }
 
 int pearl_gpu_batch_stats(const pearl_gpu_batch* b, long long* launches, int* grid_blocks, int* group_blocks,

@@ -117,8 +117,11 @@ EXPORTS = [
     "pearl_gpu_selftest_division", "pearl_gpu_advance_noalloc", "pearl_gpu_smooth_interface",
     "pearl_gpu_mixture_sums", "pearl_gpu_init_composition", "pearl_gpu_batch_create", "pearl_gpu_batch_destroy",
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
-    "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient",
+    "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
+    "pearl_gpu_batch_set_precision",
 ]
+
+PRECISION = {"fp64": 0, "mixed": 1}
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
           "mixture", "shift", "snapshot", "smooth", "init", "adjoint"]
@@ -169,6 +172,8 @@ def library(path: Path | None = None) -> C.CDLL:
                                             C.POINTER(PearlScalars), D, C.POINTER(PearlStepInfo), V]
     IP = C.POINTER(C.c_int)
     L.pearl_gpu_adjoint_gradient.argtypes = [V, C.c_longlong, C.c_int, DP, C.POINTER(PearlAdjointReport)]
+    L.pearl_gpu_set_precision.argtypes = [V, C.c_int]
+    L.pearl_gpu_batch_set_precision.argtypes = [V, C.c_int]
     L.pearl_gpu_batch_create.argtypes = [C.c_int, C.POINTER(PearlParams), IP, IP, C.c_int, C.c_int, C.POINTER(V)]
     L.pearl_gpu_batch_destroy.argtypes = [V]
     L.pearl_gpu_batch_destroy.restype = None
@@ -350,6 +355,10 @@ class Context:
         self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
         return bool(v.value)
 
+    def set_precision(self, precision: str) -> None:
+        """'fp64' (default, the reference's arithmetic) or 'mixed' (FP32 propose forces)."""
+        self._check(self.lib.pearl_gpu_set_precision(self.h, PRECISION[precision]))
+
     def adjoint_gradient(self, nsteps: int, checkpoint_every: int, target_alpha) -> PearlAdjointReport:
         """Gradient of sum((phi_alpha - target)^2) after nsteps w.r.t. (mobility scale, sigma,
         D_gamma); the context ends in the forward's final state."""
@@ -439,6 +448,9 @@ class Batch:
         st = (C.c_int * self.n)()
         self._check(self.lib.pearl_gpu_batch_run(self.h, C.byref(lim), reps, st))
         return list(reps), list(st)
+
+    def set_precision(self, precision: str) -> None:
+        self._check(self.lib.pearl_gpu_batch_set_precision(self.h, PRECISION[precision]))
 
     def autotune(self, steps: int = 2):
         g, t = C.c_int(), C.c_int()

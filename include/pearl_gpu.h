@@ -136,6 +136,16 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx);
 /* Run all work of this context on `stream` (a cudaStream_t; NULL = legacy default). */
 int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream);
 
+/* Arithmetic of the step.  PEARL_PRECISION_FP64 (the default) is the
+ * reference's arithmetic.  PEARL_PRECISION_MIXED evaluates the propose_phi
+ * forces, local tau and phase increment in FP32 (the chemical-potential
+ * terms expanded about mu_reference with the offset formed in FP64); the
+ * state, the projection, the implicit diffusion (PCG, residual recheck,
+ * carbon update), the mass and energy reductions and every acceptance test
+ * stay FP64.  No counterpart in the reference. */
+enum { PEARL_PRECISION_FP64 = 0, PEARL_PRECISION_MIXED = 1 };
+int pearl_gpu_set_precision(pearl_gpu_ctx* ctx, int precision);
+
 /* Replace the run parameters (same grid); invalidates cached step energies. */
 int pearl_gpu_set_params(pearl_gpu_ctx* ctx, const pearl_params* params);
 
@@ -297,6 +307,8 @@ int pearl_gpu_batch_run(pearl_gpu_batch* batch, const pearl_run_limits* limits, 
  * trial, and keeps the fastest; the choice is written to the out pointers
  * (may be NULL). */
 int pearl_gpu_batch_autotune(pearl_gpu_batch* batch, int steps, int* group_blocks, int* use_tma);
+/* pearl_gpu_set_precision for every instance. */
+int pearl_gpu_batch_set_precision(pearl_gpu_batch* batch, int precision);
 int pearl_gpu_batch_stats(const pearl_gpu_batch* batch, long long* kernel_launches, int* grid_blocks,
                           int* group_blocks, double* last_kernel_ms);
 const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* batch);
