@@ -348,7 +348,7 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
         e2e_steps += r.steps
         ctx.maybe_shift(meta["shift_trigger"], meta["shift_target"], meta["shift_gamma_carbon"])
         ctx.snapshot()
-        phi_o[...], c_o[...], mu_o[...], s_h = ctx.download()
+        _, _, _, s_h = ctx.download(out=(phi_o, c_o, mu_o))
         phi_h, phi_o = phi_o, phi_h
         c_h, c_o = c_o, c_h
         mu_h, mu_o = mu_o, mu_h
@@ -442,7 +442,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
     peak, peak_kind = measured_peak()
 
     # end to end: upload every instance from pinned host memory, run, download every instance
-    outs = [[np.empty_like(a) for a in hp] for hp in pinned]
+    outs = [[torch.empty(a.shape, dtype=torch.float64).pin_memory().numpy() for a in hp] for hp in pinned]
     scal = [b.download(i)[3] for i in range(len(ws))]
     barrier()
     t0 = time.perf_counter()
@@ -450,7 +450,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
         b.upload(i, *pinned[i], scal[i])
     reps2, _ = b.run(args.steps)
     for i in range(len(ws)):
-        phi, c, mu, scal[i] = b.download(i)
+        scal[i] = b.download(i, out=outs[i])[3]
     barrier()
     e2e_t = reduce_over_ranks(dist, time.perf_counter() - t0, "max", "cuda")
     e2e_cells = reduce_over_ranks(dist, float(sum(w.cells * r.steps for w, r in zip(ws, reps2))), "sum", "cuda")

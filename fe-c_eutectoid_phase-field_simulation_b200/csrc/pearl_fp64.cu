@@ -1865,7 +1865,7 @@ struct pearl_gpu_ctx {
     double* slab = nullptr;
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl = nullptr;  // pinned
-    double* h_stage = nullptr;  // pinned staging of one plane-set
+    double* d_stage = nullptr;  // dense device staging of one host state (5 n doubles)
     size_t stage_elems = 0;
     int grid = 0;
     long long launches = 0;
@@ -2128,70 +2128,80 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
 }
 
 int ensure_stage(pearl_gpu_ctx* ctx) {
-    if (!ctx->h_stage) PG_CUDA(ctx, cudaMallocHost(&ctx->h_stage, ctx->stage_elems * sizeof(double)));
+    if (!ctx->d_stage) PG_CUDA(ctx, cudaMalloc(&ctx->d_stage, ctx->stage_elems * sizeof(double)));
     return PEARL_OK;
 }
 
-// AoS host (ny,nx,3) + two scalar fields <-> padded SoA device planes
+// Host fields in the reference's gathered layout (phi (y,x,a) interleaved,
+// carbon and mu dense) travel as they are into a dense device staging buffer
+// [phi 3n | carbon n | mu n]; these kernels move them to and from the padded
+// SoA planes of one state set, so the host does no per-element work.
+__global__ void unpack_state_kernel(const double* __restrict__ st, long long n, int nx, int pitch,
+                                    double* p0, double* p1, double* p2, double* c, double* mu) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long y = i / nx, x = i - y * nx;
+        const size_t d = (size_t)y * pitch + x;
+        if (p0) {
+            p0[d] = st[3 * i];
+            p1[d] = st[3 * i + 1];
+            p2[d] = st[3 * i + 2];
+        }
+        if (c) c[d] = st[3 * n + i];
+        if (mu) mu[d] = st[4 * n + i];
+    }
+}
+
+__global__ void pack_state_kernel(double* __restrict__ st, long long n, int nx, int pitch, const double* p0,
+                                  const double* p1, const double* p2, const double* c, const double* mu) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const long long y = i / nx, x = i - y * nx;
+        const size_t d = (size_t)y * pitch + x;
+        if (p0) {
+            st[3 * i] = p0[d];
+            st[3 * i + 1] = p1[d];
+            st[3 * i + 2] = p2[d];
+        }
+        if (c) st[3 * n + i] = c[d];
+        if (mu) st[4 * n + i] = mu[d];
+    }
+}
+
+int stage_grid(const pearl_gpu_ctx* ctx) {
+    const long long n = (long long)ctx->nx * ctx->ny;
+    return (int)std::max(1LL, std::min<long long>((n + 255) / 256, 148LL * 16));
+}
+
 int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* carbon, const double* mu) {
     if (int rc = ensure_stage(ctx)) return rc;
     const size_t n = (size_t)ctx->nx * ctx->ny;
-    const size_t pe = plane_elems(ctx);
-    double* st = ctx->h_stage;
-    if (phi) {
-        for (int a = 0; a < 3; ++a) {
-            for (int y = 0; y < ctx->ny; ++y)
-                for (int x = 0; x < ctx->nx; ++x)
-                    st[(size_t)a * pe + (size_t)y * ctx->pitch + x] = phi[((size_t)y * ctx->nx + x) * 3 + a];
-        }
-    }
+    double* st = ctx->d_stage;
+    if (phi) PG_CUDA(ctx, cudaMemcpyAsync(st, phi, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     if (carbon)
-        for (int y = 0; y < ctx->ny; ++y)
-            std::memcpy(st + 3 * pe + (size_t)y * ctx->pitch, carbon + (size_t)y * ctx->nx, sizeof(double) * ctx->nx);
-    if (mu)
-        for (int y = 0; y < ctx->ny; ++y)
-            std::memcpy(st + 4 * pe + (size_t)y * ctx->pitch, mu + (size_t)y * ctx->nx, sizeof(double) * ctx->nx);
-    (void)n;
-    if (phi)
-        for (int a = 0; a < 3; ++a)
-            PG_CUDA(ctx, cudaMemcpyAsync(ctx->B.phi[set][a], st + (size_t)a * pe, pe * sizeof(double),
-                                         cudaMemcpyHostToDevice, ctx->stream));
-    if (carbon)
-        PG_CUDA(ctx, cudaMemcpyAsync(ctx->B.c[set], st + 3 * pe, pe * sizeof(double), cudaMemcpyHostToDevice,
-                                     ctx->stream));
-    if (mu)
-        PG_CUDA(ctx, cudaMemcpyAsync(ctx->B.mu[set], st + 4 * pe, pe * sizeof(double), cudaMemcpyHostToDevice,
-                                     ctx->stream));
+        PG_CUDA(ctx, cudaMemcpyAsync(st + 3 * n, carbon, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (mu) PG_CUDA(ctx, cudaMemcpyAsync(st + 4 * n, mu, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    unpack_state_kernel<<<stage_grid(ctx), 256, 0, ctx->stream>>>(
+        st, (long long)n, ctx->nx, ctx->pitch, phi ? ctx->B.phi[set][0] : nullptr, ctx->B.phi[set][1],
+        ctx->B.phi[set][2], carbon ? ctx->B.c[set] : nullptr, mu ? ctx->B.mu[set] : nullptr);
+    ctx->launches++;
+    PG_CUDA(ctx, cudaGetLastError());
     PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return PEARL_OK;
 }
 
 int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, double* mu) {
     if (int rc = ensure_stage(ctx)) return rc;
-    const size_t pe = plane_elems(ctx);
-    double* st = ctx->h_stage;
-    if (phi)
-        for (int a = 0; a < 3; ++a)
-            PG_CUDA(ctx, cudaMemcpyAsync(st + (size_t)a * pe, ctx->B.phi[set][a], pe * sizeof(double),
-                                         cudaMemcpyDeviceToHost, ctx->stream));
+    const size_t n = (size_t)ctx->nx * ctx->ny;
+    double* st = ctx->d_stage;
+    pack_state_kernel<<<stage_grid(ctx), 256, 0, ctx->stream>>>(
+        st, (long long)n, ctx->nx, ctx->pitch, phi ? ctx->B.phi[set][0] : nullptr, ctx->B.phi[set][1],
+        ctx->B.phi[set][2], carbon ? ctx->B.c[set] : nullptr, mu ? ctx->B.mu[set] : nullptr);
+    ctx->launches++;
+    PG_CUDA(ctx, cudaGetLastError());
+    if (phi) PG_CUDA(ctx, cudaMemcpyAsync(phi, st, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (carbon)
-        PG_CUDA(ctx, cudaMemcpyAsync(st + 3 * pe, ctx->B.c[set], pe * sizeof(double), cudaMemcpyDeviceToHost,
-                                     ctx->stream));
-    if (mu)
-        PG_CUDA(ctx, cudaMemcpyAsync(st + 4 * pe, ctx->B.mu[set], pe * sizeof(double), cudaMemcpyDeviceToHost,
-                                     ctx->stream));
+        PG_CUDA(ctx, cudaMemcpyAsync(carbon, st + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (mu) PG_CUDA(ctx, cudaMemcpyAsync(mu, st + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (phi)
-        for (int y = 0; y < ctx->ny; ++y)
-            for (int x = 0; x < ctx->nx; ++x)
-                for (int a = 0; a < 3; ++a)
-                    phi[((size_t)y * ctx->nx + x) * 3 + a] = st[(size_t)a * pe + (size_t)y * ctx->pitch + x];
-    if (carbon)
-        for (int y = 0; y < ctx->ny; ++y)
-            std::memcpy(carbon + (size_t)y * ctx->nx, st + 3 * pe + (size_t)y * ctx->pitch, sizeof(double) * ctx->nx);
-    if (mu)
-        for (int y = 0; y < ctx->ny; ++y)
-            std::memcpy(mu + (size_t)y * ctx->nx, st + 4 * pe + (size_t)y * ctx->pitch, sizeof(double) * ctx->nx);
     return PEARL_OK;
 }
 
@@ -2290,7 +2300,7 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     std::memset(ctx->h_ctl, 0, sizeof(Ctl));
     ctx->B.ctl = ctx->d_ctl;
     if (ctx->use_tma && !build_tensor_maps(ctx)) ctx->use_tma = false;
-    ctx->stage_elems = 5 * pe;  // pinned staging is allocated at the first host transfer
+    ctx->stage_elems = 5 * (size_t)nx * ny;  // device staging is allocated at the first host transfer
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
         return bail(PEARL_ERR_CUDA);
     if (cudaMemcpy(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -2306,7 +2316,7 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
     if (ctx->slab) cudaFree(ctx->slab);
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
-    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     delete ctx;

@@ -264,10 +264,15 @@ class Context:
             s = scalars if isinstance(scalars, PearlScalars) else PearlScalars.from_dict(scalars)
         self._check(self.lib.pearl_gpu_upload(self.h, _p(phi), _p(carbon), _p(mu), C.byref(s) if s else None))
 
-    def download(self):
-        phi = np.empty((self.ny, self.nx, 3))
-        carbon = np.empty((self.ny, self.nx))
-        mu = np.empty((self.ny, self.nx))
+    def download(self, out=None):
+        """(phi, carbon, mu, scalars); `out` = (phi, carbon, mu) arrays to write into
+        (e.g. pinned host buffers), else new arrays."""
+        if out is None:
+            phi = np.empty((self.ny, self.nx, 3))
+            carbon = np.empty((self.ny, self.nx))
+            mu = np.empty((self.ny, self.nx))
+        else:
+            phi, carbon, mu = out
         s = PearlScalars()
         self._check(self.lib.pearl_gpu_download(self.h, _p(phi), _p(carbon), _p(mu), C.byref(s)))
         return phi, carbon, mu, s
@@ -431,11 +436,14 @@ class Batch:
         self._check(self.lib.pearl_gpu_batch_upload(self.h, i, _p(phi), _p(carbon), _p(mu),
                                                     C.byref(s) if s else None))
 
-    def download(self, i: int):
+    def download(self, i: int, out=None):
         nx, ny = self.shapes[i]
-        phi = np.empty((ny, nx, 3))
-        carbon = np.empty((ny, nx))
-        mu = np.empty((ny, nx))
+        if out is None:
+            phi = np.empty((ny, nx, 3))
+            carbon = np.empty((ny, nx))
+            mu = np.empty((ny, nx))
+        else:
+            phi, carbon, mu = out
         s = PearlScalars()
         self._check(self.lib.pearl_gpu_batch_download(self.h, i, _p(phi), _p(carbon), _p(mu), C.byref(s)))
         return phi, carbon, mu, s
