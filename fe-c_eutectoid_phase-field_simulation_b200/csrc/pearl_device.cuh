@@ -66,6 +66,9 @@ struct DevParams {
 // '/' by pearl_gpu_selftest_division).  Zero and non-finite numerators keep
 // the sign/special value of a*rb.  Falls back to '/' when the host found a
 // divisor outside the normal range.
+// The zero / non-finite test reads the bit patterns with integer operations,
+// which leaves the FP64 pipe to the arithmetic: a == +-0 when its magnitude
+// bits are all zero, q0 is Inf or NaN when its exponent field is all ones.
 __device__ __forceinline__ double div_by(const DevParams& P, double a, double b, double rb) {
     if (!P.exact_div) return a / b;
     const double q0 = a * rb;
@@ -73,7 +76,9 @@ __device__ __forceinline__ double div_by(const DevParams& P, double a, double b,
     double q = fma(r, rb, q0);
     r = fma(-q, b, a);
     q = fma(r, rb, q);
-    return (a == 0.0 || !isfinite(q0)) ? q0 : q;
+    const int ah = __double2hiint(a), al = __double2loint(a), qh = __double2hiint(q0);
+    const bool special = (((ah & 0x7fffffff) | al) == 0) | ((qh & 0x7ff00000) == 0x7ff00000);
+    return special ? q0 : q;
 }
 
 // Device buffers: two state sets (current / trial, selected by Ctl::cur) and
