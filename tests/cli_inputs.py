@@ -89,6 +89,15 @@ def case_moving_window():
         ("shift_target", "40e-9")]
 
 
+def case_smoke():
+    """The key-values of the reference's start-up check examples/fe_c_phase_diagram_10K_smoke.in
+    (137x250, sharp_smooth, to 0.015 microseconds: ~5,500 adaptive steps)."""
+    return PHASE_DIAGRAM_10K + grid(137, 250, dt="1.5e-11", end="1.5e-8", out="2.5e-8") + COMMON + [
+        ("initialization", "sharp_smooth"), ("seed_height", "58.59e-9"), ("theta_columns", "17"),
+        ("gamma_carbon", "0.034458832049305582"), ("smooth_steps", "100"), ("smooth_min_steps", "100"),
+        ("smooth_energy_rtol", "1e-10"), ("smooth_max_phase_change", "0.02")]
+
+
 VALID = {
     "sharp_smooth": case_sharp_smooth,
     "lamella_linear_gp": case_lamella_linear_gp,

@@ -146,3 +146,34 @@ def test_cli_restart_from_reference_checkpoint(cli, tmp_path):
     a, b = read_container(outs["gpu"] / "checkpoint.h5"), read_container(outs["ref"] / "checkpoint.h5")
     assert np.abs(a["alpha"] - b["alpha"]).max() <= 1e-10
     assert np.abs(a["mu"] - b["mu"]).max() <= 1e-5
+
+
+@pytest.mark.gpu
+def test_cli_smoke_run_matches_reference(cli, tmp_path):
+    """Known answer: the reference's start-up check (137x250, sharp_smooth, to
+    0.015 microseconds, ~5,500 adaptive steps with ~750 rejections), run by the
+    reference program here (make_smoke_golden.py), is reproduced step for step:
+    same accepted steps, rejections and total CG iterations, final fields within
+    the FP64 tolerances."""
+    from golden.make_cli_golden import read_container
+
+    ref = json.loads((GOLDEN / "smoke_golden.json").read_text())
+    p, out = _run(cli, cli_inputs.case_smoke(), [], tmp_path, "smoke")
+    assert p.returncode == 0, p.stderr
+    assert sorted(x.name for x in out.iterdir()) == ref["files"]
+    assert (out / "COMPLETED.txt").read_text() == ref["completed"]
+    head, rows = _csv((out / "diagnostics.csv").read_text())
+    rhead, rrows = _csv(ref["diagnostics"])
+    assert head == rhead and len(rows) == len(rrows)
+    for r, g in zip(rows, rrows):
+        for k in ("time", "step", "dt_next", "cg_last", "cg_peak", "rejected"):
+            assert r[k] == g[k], k
+        for k in ("mu_min", "mu_max"):
+            assert abs(r[k] - g[k]) <= 1e-5, k
+    fields = read_container(out / "checkpoint.h5")
+    ref_fields = np.load(GOLDEN / "smoke_fields.npz")
+    for a in ("alpha", "theta", "gamma"):
+        assert np.abs(fields[a] - ref_fields[a]).max() <= 1e-10
+    assert np.abs(fields["mu"] - ref_fields["mu"]).max() <= 1e-5
+    c, c_ref = fields["carbon"], ref_fields["carbon"]
+    assert abs(c.sum() - c_ref.sum()) <= 1e-12 * abs(c_ref.sum())
