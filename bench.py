@@ -388,6 +388,40 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
     ctx.close()
 
 
+def _cpu_sweep_task(task):
+    """One sweep instance on one host core: `steps` whole steps of the reference solver
+    (oracle/_ref, else the C restatement).  Returns (cell-updates, kind)."""
+    i, seed, steps = task
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    w = workloads.sweep_one(i, seed)
+    ref = pyoracle.reference()
+    lib, kind = (ref, "reference") if ref is not None else (pyoracle.port(), "port")
+    phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    s = pyoracle.scalars_from(w.scalars)
+    out = lib.advance_n(w.params, phi, c, mu, s, steps)
+    if out[0] != 0:
+        raise RuntimeError(f"CPU sweep instance {i} failed: {out[1]}")
+    return w.cells * steps, kind
+
+
+def cpu_sweep_sample(n: int, seed: int, steps: int):
+    """The sweep on all host cores: one process per core, each running whole
+    instances (`steps` steps each) of the same n instances.  Processes are
+    spawned (the parent holds a CUDA context).  Returns (rate, kind, cores, secs)."""
+    import multiprocessing as mp
+
+    cores = max(1, os.cpu_count() or 1)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        pool.map(_cpu_sweep_task, [(0, seed, 1)] * cores)  # start-up (imports, oracle load) untimed
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_sweep_task, [(i, seed, steps) for i in range(n)], chunksize=1)
+        secs = time.perf_counter() - t0
+    return sum(r[0] for r in res) / secs, res[0][1], cores, secs
+
+
 def sweep_arm(args, rank: int, world: int, dist) -> None:
     """Batched parameter sweep: --instances independent domains (2 lamellar pairs of
     spacing U{16..96} across x, growth length U{64..1024}, ferrite fraction
@@ -455,6 +489,12 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
     e2e_t = reduce_over_ranks(dist, time.perf_counter() - t0, "max", "cuda")
     e2e_cells = reduce_over_ranks(dist, float(sum(w.cells * r.steps for w, r in zip(ws, reps2))), "sum", "cuda")
     state_bytes = 40 * cells
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, secs = cpu_sweep_sample(len(ws), rank, 10)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"all {len(ws)} instances, 10 whole steps each, one process per host core "
+                         f"({secs:.1f} s wall)", "cpu": _cpu_model()}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -472,7 +512,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_batch_kernel (persistent FP64 step, block groups)",
                          "algorithmic_bytes_per_launch": algo_bytes},
-            "cpu_baseline": None,
+            "cpu_baseline": cpu,
             "e2e": {"value": e2e_cells / e2e_t, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps,
                     "step": f"upload all instances, {args.steps} steps each in one launch, download all"},

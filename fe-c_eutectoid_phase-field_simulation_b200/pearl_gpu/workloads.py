@@ -240,10 +240,15 @@ def sweep_instance(i: int, rng: np.random.Generator, dt: float = 4e-12) -> Workl
     return _finish(f"sweep_{i}_{nx}x{ny}", nx, ny, params, phi, meta)
 
 
+def sweep_one(i: int, seed: int = 0) -> Workload:
+    """Instance i of the sweep drawn from `seed` (its own stream, so any instance
+    can be built alone)."""
+    return sweep_instance(i, np.random.default_rng([seed, i]))
+
+
 def sweep(n: int = 256, seed: int = 0) -> list[Workload]:
     """n sweep instances drawn from one seed (the batched-sweep workload)."""
-    rng = np.random.default_rng(seed)
-    return [sweep_instance(i, rng) for i in range(n)]
+    return [sweep_one(i, seed) for i in range(n)]
 
 
 ADJOINT_PARAMETERS = ("mobility", "sigma", "D_gamma")
