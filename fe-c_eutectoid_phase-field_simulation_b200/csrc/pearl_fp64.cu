@@ -1846,6 +1846,11 @@ __global__ void division_selftest_kernel(const double* a, const double* b, const
     if (bad) atomicAdd(mismatches, bad);
 }
 
+// Self-test of the bounded grid-barrier wait: every block waits for one
+// arrival more than the grid has, so no wait can complete; each gives up after
+// kBarrierTimeoutNs and records PEARL_ERR_DEVICE_WAIT.
+__global__ void wait_limit_selftest_kernel(Ctl* ctl) { grid_barrier(ctl, gridDim.x + 1u); }
+
 #include "pearl_adjoint.cuh"
 
 }  // namespace pearl_gpu
@@ -2593,6 +2598,37 @@ int pearl_gpu_selftest_division(int device, const double* a, const double* b, lo
     cudaFree(drb);
     cudaFree(dm);
     return rc;
+}
+
+int pearl_gpu_selftest_wait_limit(pearl_gpu_ctx* ctx, int* status, double* waited_ms) {
+    if (!ctx || !status) return PEARL_ERR_INVALID_ARGUMENT;
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    ctx->h_ctl->status = 0;
+    ctx->h_ctl->why = 0;
+    ctx->h_ctl->bar_count = 0;
+    int rc = push_ctl(ctx);
+    if (rc) return rc;
+    Ctl* ctl = ctx->d_ctl;
+    void* kargs[] = {&ctl};
+    PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)wait_limit_selftest_kernel, dim3(ctx->grid),
+                                             dim3(kThreads), kargs, 0, ctx->stream));
+    ctx->launches++;
+    PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    rc = pull_ctl(ctx);
+    if (rc) return rc;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    if (waited_ms) *waited_ms = ms;
+    *status = ctx->h_ctl->status;
+    // leave the barrier words and status as a fresh context has them
+    ctx->h_ctl->status = 0;
+    ctx->h_ctl->why = 0;
+    ctx->h_ctl->bar_count = 0;
+    rc = push_ctl(ctx);
+    if (rc) return rc;
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PEARL_OK;
 }
 
 int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts) {

@@ -118,7 +118,7 @@ EXPORTS = [
     "pearl_gpu_mixture_sums", "pearl_gpu_init_composition", "pearl_gpu_batch_create", "pearl_gpu_batch_destroy",
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
-    "pearl_gpu_batch_set_precision",
+    "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit",
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -173,6 +173,7 @@ def library(path: Path | None = None) -> C.CDLL:
     IP = C.POINTER(C.c_int)
     L.pearl_gpu_adjoint_gradient.argtypes = [V, C.c_longlong, C.c_int, DP, C.POINTER(PearlAdjointReport)]
     L.pearl_gpu_set_precision.argtypes = [V, C.c_int]
+    L.pearl_gpu_selftest_wait_limit.argtypes = [V, C.POINTER(C.c_int), DP]
     L.pearl_gpu_batch_set_precision.argtypes = [V, C.c_int]
     L.pearl_gpu_batch_create.argtypes = [C.c_int, C.POINTER(PearlParams), IP, IP, C.c_int, C.c_int, C.POINTER(V)]
     L.pearl_gpu_batch_destroy.argtypes = [V]
@@ -359,6 +360,12 @@ class Context:
         v = C.c_int()
         self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
         return bool(v.value)
+
+    def selftest_wait_limit(self):
+        """(status, device ms) of a grid barrier that cannot complete (see pearl_gpu.h)."""
+        st, ms = C.c_int(), D()
+        self._check(self.lib.pearl_gpu_selftest_wait_limit(self.h, C.byref(st), C.byref(ms)))
+        return st.value, ms.value
 
     def set_precision(self, precision: str) -> None:
         """'fp64' (default, the reference's arithmetic) or 'mixed' (FP32 propose forces)."""

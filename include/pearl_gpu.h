@@ -223,6 +223,14 @@ int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* count
 int pearl_gpu_selftest_division(int device, const double* a, const double* b, long long n,
                                 unsigned long long* mismatches);
 
+/* Self-test of the bounded device waits, on this context's grid and control
+ * block: launches a grid barrier that waits for one block more than the grid
+ * has, so every block must give up after the barrier's time limit (4 s).
+ * *status receives the recorded status (PEARL_ERR_DEVICE_WAIT when the limit
+ * works), *waited_ms (may be NULL) the device time; the context is left ready
+ * for further calls.  No reference counterpart. */
+int pearl_gpu_selftest_wait_limit(pearl_gpu_ctx* ctx, int* status, double* waited_ms);
+
 /* One accepted step (as pearl_gpu_advance) for callers that cannot allocate
  * device memory: code whose GPU memory is owned by another allocator (a
  * framework's caching pool or a fixed memory budget) and latency-critical

@@ -213,3 +213,26 @@ def test_large_domain_properties(gpu_lib):
     assert abs(m1 - m0) <= 1e-11 * abs(m0)
     assert e1 <= e0
     assert all(i.energy_change <= 1e-12 * abs(e0) + 1e-20 for i in infos)
+
+
+def test_bounded_wait_reports_and_recovers(gpu_lib):
+    """A grid barrier that cannot complete gives up after its limit (4 s) with
+    PEARL_ERR_DEVICE_WAIT instead of hanging, and the context keeps working:
+    the next step equals a fresh context's step bitwise."""
+    import pearl_gpu
+    from pearl_gpu import workloads
+
+    w = workloads.scaled(64, 48, seed=5, front=12.0)
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as ctx:
+        ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
+        status, ms = ctx.selftest_wait_limit()
+        assert status == 9  # PEARL_ERR_DEVICE_WAIT
+        assert 3900.0 <= ms <= 30000.0
+        ctx.advance()
+        got = ctx.download()
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as ref:
+        ref.upload(w.phi, w.carbon, w.mu, w.scalars)
+        ref.advance()
+        want = ref.download()
+    for a, b in zip(got[:3], want[:3]):
+        assert np.array_equal(a, b)
