@@ -505,6 +505,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
                        "instances": len(ws), "cells": cells, "group_blocks": st_["group_blocks"],
                        "grid_blocks": st_["grid"], "autotuned": tuned is not None,
                        "tma": None if tuned is None else tuned[1],
+                       "tile": None if tuned is None else f"{32 * tuned[2]}x{16 // tuned[2]}",
                        "l2": "inputs larger than L2 (state 40 B/cell = %.0f MB)" % (40 * cells / 1e6),
                        "parallelism": f"replicas x{world}", "bytes_per_cell_update": "80 + 64*n_CG"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

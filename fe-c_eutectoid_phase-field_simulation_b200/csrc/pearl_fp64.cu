@@ -1933,6 +1933,16 @@ double host_psi(const pearl_params* p, int a, double mu) {
     return std::fma(-0.25 / p->A[a], d * d, p->C[a]);
 }
 
+// Tile of (32 << wx) x (2 << (3 - wx)) cells: 2^wx warps side by side in x.
+void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2) {
+    DevParams& P = ctx->P;
+    P.warps_x_log2 = wx_log2;
+    const int tile_w = 32 << wx_log2, tile_h = 2 << (3 - wx_log2);
+    P.ntx = (ctx->nx + tile_w - 1) / tile_w;
+    P.nty = (ctx->ny + tile_h - 1) / tile_h;
+    P.ntiles = P.ntx * P.nty;
+}
+
 void fill_dev_params(pearl_gpu_ctx* ctx) {
     const pearl_params* p = &ctx->params;
     DevParams& P = ctx->P;
@@ -1946,11 +1956,7 @@ void fill_dev_params(pearl_gpu_ctx* ctx) {
         const int w = std::atoi(e);
         wx_log2 = w >= 8 ? 3 : w >= 4 ? 2 : w >= 2 ? 1 : 0;
     }
-    P.warps_x_log2 = wx_log2;
-    const int tile_w = 32 << wx_log2, tile_h = 2 << (3 - wx_log2);
-    P.ntx = (ctx->nx + tile_w - 1) / tile_w;
-    P.nty = (ctx->ny + tile_h - 1) / tile_h;
-    P.ntiles = P.ntx * P.nty;
+    set_tile_shape(ctx, wx_log2);
     P.dx = p->dx;
     P.dy = p->dy;
     P.dx2 = p->dx * p->dx;
@@ -2858,7 +2864,9 @@ struct pearl_gpu_batch {
     Ctl* d_group_ctl = nullptr;
     double* d_group_part = nullptr;
     int per_sm = 0, sms = 0, grid = 0, group_blocks = 0, ngroups = 0;
-    bool use_tma = true;
+    bool use_tma = true;      // TMA staging in use (needs the 32x16 tile)
+    bool tma_capable = true;  // tensor maps of every instance encoded and the shared memory granted
+    int tile_wx = 0;          // tile shape of every instance: 2^tile_wx warps side by side in x
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0;
@@ -2878,15 +2886,19 @@ int bfail(pearl_gpu_batch* b, int status, const std::string& msg) {
         if (e_ != cudaSuccess) return bfail(b, PEARL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// Split the cooperative grid into groups of `gb` blocks and hand out the
-// instances longest-first to the least-loaded group (cost ~ cells).
-int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma) {
+// Give every instance the tile shape `wx`, split the cooperative grid into
+// groups of `gb` blocks and hand out the instances longest-first to the
+// least-loaded group (cost ~ cells).  TMA staging needs the 32x16 tile.
+int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma, int wx) {
     const int max_grid = b->per_sm * b->sms;
     if (gb < 1 || gb > max_grid) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid group size");
+    if (wx < 0 || wx > 3) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid tile shape");
     b->group_blocks = gb;
     b->ngroups = max_grid / gb;
     b->grid = b->ngroups * gb;
-    b->use_tma = use_tma;
+    b->tile_wx = wx;
+    b->use_tma = use_tma && wx == 0 && b->tma_capable;
+    for (auto* c : b->inst) set_tile_shape(c, wx);
     std::vector<int> idx(b->n);
     for (int i = 0; i < b->n; ++i) idx[i] = i;
     std::sort(idx.begin(), idx.end(), [&](int x, int y) {
@@ -3028,7 +3040,8 @@ int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, con
                                                       tma ? kTmaSmemBytes : 0) != cudaSuccess ||
         b->per_sm < 1)
         return bail(PEARL_ERR_CUDA);
-    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : 4, tma);
+    b->tma_capable = tma;
+    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : 4, tma, 0);
     if (rc) return bail(rc);
     *out = b;
     return PEARL_OK;
@@ -3072,7 +3085,7 @@ int pearl_gpu_batch_run(pearl_gpu_batch* b, const pearl_run_limits* limits, pear
     return PEARL_OK;
 }
 
-int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, int* use_tma) {
+int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, int* use_tma, int* tile_warps_x) {
     if (!b || steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
     PB_CUDA(b, cudaSetDevice(b->device));
     // back up every instance's current state (5 planes) and control block
@@ -3092,16 +3105,26 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
     // the instances' host control blocks are authoritative (uploads update them)
     std::vector<Ctl> saved(b->n);
     for (int i = 0; i < b->n; ++i) saved[i] = *b->inst[i]->h_ctl;
-    const bool can_tma = b->use_tma;
     double best_ms = 1e300;
-    int best_gb = b->group_blocks;
+    int best_gb = b->group_blocks, best_wx = b->tile_wx;
     bool best_tma = b->use_tma;
     const int cands[] = {1, 2, 4, 8, 16};
     pearl_run_limits L{1, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
-    for (int tma = can_tma ? 1 : 0; tma >= 0; --tma) {
+    // tile shapes 32x16 (with and without TMA staging), 64x8 and 128x4
+    struct Shape {
+        int wx;
+        bool tma;
+    };
+    std::vector<Shape> shapes;
+    if (b->tma_capable) shapes.push_back({0, true});
+    shapes.push_back({0, false});
+    shapes.push_back({1, false});
+    shapes.push_back({2, false});
+    for (const Shape& sh : shapes) {
+        const int tma = sh.tma ? 1 : 0;
         for (int gb : cands) {
             if (gb > b->per_sm * b->sms) continue;
-            int rc = batch_configure(b, gb, tma != 0);
+            int rc = batch_configure(b, gb, tma != 0, sh.wx);
             double ms = 0;
             for (int s = 0; rc == PEARL_OK && s < steps; ++s) {
                 rc = batch_launch(b, L);
@@ -3125,14 +3148,24 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
                 best_ms = ms;
                 best_gb = gb;
                 best_tma = tma != 0;
+                best_wx = sh.wx;
             }
         }
     }
     release();
-    const int rc = batch_configure(b, best_gb, best_tma);
+    const int rc = batch_configure(b, best_gb, best_tma, best_wx);
     if (group_blocks) *group_blocks = best_gb;
     if (use_tma) *use_tma = best_tma ? 1 : 0;
+    if (tile_warps_x) *tile_warps_x = 1 << best_wx;
     return rc;
+}
+
+int pearl_gpu_batch_configure(pearl_gpu_batch* b, int group_blocks, int use_tma, int tile_warps_x) {
+    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
+    const int wx = tile_warps_x == 1 ? 0 : tile_warps_x == 2 ? 1 : tile_warps_x == 4 ? 2 : tile_warps_x == 8 ? 3 : -1;
+    if (wx < 0) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "tile_warps_x must be 1, 2, 4 or 8");
+    PB_CUDA(b, cudaSetDevice(b->device));
+    return batch_configure(b, group_blocks, use_tma != 0, wx);
 }
 
 int pearl_gpu_batch_set_precision(pearl_gpu_batch* b, int precision) {
@@ -3141,7 +3174,7 @@ int pearl_gpu_batch_set_precision(pearl_gpu_batch* b, int precision) {
         const int rc = pearl_gpu_set_precision(c, precision);
         if (rc) return bfail(b, rc, "invalid precision");
     }
-    return batch_configure(b, b->group_blocks, b->use_tma);
+    return batch_configure(b, b->group_blocks, b->use_tma, b->tile_wx);
 }
 
 int pearl_gpu_batch_stats(const pearl_gpu_batch* b, long long* launches, int* grid_blocks, int* group_blocks,

@@ -118,7 +118,7 @@ EXPORTS = [
     "pearl_gpu_mixture_sums", "pearl_gpu_init_composition", "pearl_gpu_batch_create", "pearl_gpu_batch_destroy",
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
-    "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit",
+    "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit", "pearl_gpu_batch_configure",
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -181,7 +181,8 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_batch_upload.argtypes = [V, C.c_int, DP, DP, DP, C.POINTER(PearlScalars)]
     L.pearl_gpu_batch_download.argtypes = [V, C.c_int, DP, DP, DP, C.POINTER(PearlScalars)]
     L.pearl_gpu_batch_run.argtypes = [V, C.POINTER(PearlRunLimits), C.POINTER(PearlRunReport), IP]
-    L.pearl_gpu_batch_autotune.argtypes = [V, C.c_int, IP, IP]
+    L.pearl_gpu_batch_autotune.argtypes = [V, C.c_int, IP, IP, IP]
+    L.pearl_gpu_batch_configure.argtypes = [V, C.c_int, C.c_int, C.c_int]
     L.pearl_gpu_batch_stats.argtypes = [V, C.POINTER(C.c_longlong), IP, IP, DP]
     L.pearl_gpu_batch_last_error.argtypes = [V]
     L.pearl_gpu_batch_last_error.restype = C.c_char_p
@@ -467,10 +468,14 @@ class Batch:
     def set_precision(self, precision: str) -> None:
         self._check(self.lib.pearl_gpu_batch_set_precision(self.h, PRECISION[precision]))
 
+    def configure(self, group_blocks: int, use_tma: bool = True, tile_warps_x: int = 1) -> None:
+        self._check(self.lib.pearl_gpu_batch_configure(self.h, group_blocks, int(use_tma), tile_warps_x))
+
     def autotune(self, steps: int = 2):
-        g, t = C.c_int(), C.c_int()
-        self._check(self.lib.pearl_gpu_batch_autotune(self.h, steps, C.byref(g), C.byref(t)))
-        return g.value, bool(t.value)
+        """Chooses (group blocks, TMA staging, warps side by side in x of the tile)."""
+        g, t, w = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.pearl_gpu_batch_autotune(self.h, steps, C.byref(g), C.byref(t), C.byref(w)))
+        return g.value, bool(t.value), w.value
 
     def stats(self):
         n, grid, gb, ms = C.c_longlong(), C.c_int(), C.c_int(), D()

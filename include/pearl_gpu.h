@@ -310,13 +310,20 @@ int pearl_gpu_batch_download(pearl_gpu_batch* batch, int i, double* phi_aos3, do
  * PEARL_OK unless the launch itself failed. */
 int pearl_gpu_batch_run(pearl_gpu_batch* batch, const pearl_run_limits* limits, pearl_run_report* reports,
                         int* status);
-/* Times `steps` one-step launches for each group size in {1,2,4,8,16} with
- * and without TMA staging, restoring every instance's state after each
- * trial, and keeps the fastest; the choice is written to the out pointers
- * (may be NULL). */
-int pearl_gpu_batch_autotune(pearl_gpu_batch* batch, int steps, int* group_blocks, int* use_tma);
+/* Times `steps` one-step launches for each group size in {1,2,4,8,16} and
+ * each tile shape (32x16 cells with and without TMA staging, 64x8, 128x4),
+ * restoring every instance's state after each trial, and keeps the fastest;
+ * the choice is written to the out pointers (may be NULL; tile_warps_x = warps
+ * side by side in x: 1, 2 or 4).  The tile shape changes which block owns
+ * which cells, hence the order of the sums, not the arithmetic of a cell. */
+int pearl_gpu_batch_autotune(pearl_gpu_batch* batch, int steps, int* group_blocks, int* use_tma,
+                             int* tile_warps_x);
 /* pearl_gpu_set_precision for every instance. */
 int pearl_gpu_batch_set_precision(pearl_gpu_batch* batch, int precision);
+/* Sets the configuration pearl_gpu_batch_autotune would choose: blocks per
+ * group, TMA staging (used only with tile_warps_x = 1) and the tile shape
+ * (tile_warps_x warps side by side in x: 1, 2, 4 or 8). */
+int pearl_gpu_batch_configure(pearl_gpu_batch* batch, int group_blocks, int use_tma, int tile_warps_x);
 int pearl_gpu_batch_stats(const pearl_gpu_batch* batch, long long* kernel_launches, int* grid_blocks,
                           int* group_blocks, double* last_kernel_ms);
 const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* batch);

@@ -124,16 +124,39 @@ def test_batch_instance_error_is_local(gpu_lib):
 def test_batch_autotune_keeps_state(gpu_lib):
     ws = _cases()
     with _batch(ws, 4) as a:
-        gb, tma = a.autotune(steps=1)
-        assert gb in (1, 2, 4, 8, 16)
+        gb, tma, wx = a.autotune(steps=1)
+        assert gb in (1, 2, 4, 8, 16) and wx in (1, 2, 4)
         assert a.stats()["group_blocks"] == gb
         assert a.run(10)[1] == [0] * len(ws)
         fa = [a.download(i) for i in range(len(ws))]
     with _batch(ws, gb) as b:
+        b.configure(gb, not tma, wx)  # TMA staging moves data only: it changes no value
         b.run(10)
         fb = [b.download(i) for i in range(len(ws))]
     for x, y in zip(fa, fb):
         assert x[3].step == y[3].step == 10
-        # same group size; TMA staging does not change any value
         for u, v in zip(x[:3], y[:3]):
             assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("wx", [2, 4])
+def test_batch_tile_shapes_match_oracle(gpu_lib, port, wx):
+    """Wider tiles change only which block owns which cells (the order of sums)."""
+    from oracle import pyoracle
+
+    ws = _cases()
+    n = 12
+    with _batch(ws, 4) as b:
+        b.configure(4, False, wx)
+        reps, st = b.run(n)
+        assert st == [0] * len(ws)
+        got = [b.download(i) for i in range(len(ws))]
+    for w, (phi, c, mu, s) in zip(ws, got):
+        phi_o, c_o, mu_o = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+        so = pyoracle.scalars_from(w.scalars)
+        rc, why, done, _ = port.advance_n(w.params, phi_o, c_o, mu_o, so, n)
+        assert rc == 0 and done == n, why
+        assert s.rejected == so.rejected and s.step == so.step
+        assert np.abs(phi - phi_o).max() <= PHI_TOL
+        assert np.abs(mu - mu_o).max() <= MU_TOL
+        assert abs(c.sum() - c_o.sum()) <= MASS_RTOL * abs(c_o.sum())
