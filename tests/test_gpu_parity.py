@@ -154,3 +154,24 @@ def test_run_matches_advance(gpu_lib):
     assert rep.steps == 12
     for x, y in zip(fa[:3], fb[:3]):
         assert np.array_equal(x, y)
+
+
+EDGE_SIZES = [(3, 2, 1.0), (3, 5, 2.0), (4, 3, 1.5), (31, 17, 6.0), (33, 16, 8.0), (65, 33, 10.0)]
+
+
+@pytest.mark.parametrize("nx,ny,front", EDGE_SIZES)
+def test_smallest_and_ragged_domains(gpu_lib, port, nx, ny, front):
+    """The smallest domains the reference accepts (nx >= 3, ny >= 2) and widths
+    and heights just off the 32x16 tile: propose_phi bitwise, then 8 coupled
+    steps against the oracle with the same decisions."""
+    from pearl_gpu import workloads
+
+    w = workloads.scaled(nx, ny, seed=3, front=front)
+    with _ctx(w) as ctx:
+        change = ctx.propose_phi(4e-12)
+        trial, _, _ = ctx.download_trial()
+    rc, trial_o, change_o = port.propose_phi(w.params, w.phi, w.mu, 4e-12)
+    assert rc == 0 and change == change_o
+    assert np.array_equal(trial, trial_o)
+    with _ctx(w) as ctx:
+        _compare_run(ctx, w, port, 8)
