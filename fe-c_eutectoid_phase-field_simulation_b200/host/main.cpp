@@ -24,6 +24,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "config.hpp"
@@ -50,6 +51,62 @@ struct Gpu {
             throw std::runtime_error(msg && *msg ? msg : pearl_gpu_status_string(rc));
         }
     }
+};
+
+// Frame output on a background thread, so the device launches up to the next
+// output time overlap the file writing.  One frame is in flight at a time:
+// wait() joins it, rethrows its error, and only then emits its diagnostics and
+// console lines, so files and lines appear in the reference's order (frame,
+// then its log line) and a failed write logs nothing for that frame.
+class FrameWriter {
+  public:
+    explicit FrameWriter(std::ofstream& log) : log_(log) {}
+    // on an error elsewhere the frame in flight still completes and, if it was
+    // written, its lines appear before the error message, as in the reference
+    ~FrameWriter() {
+        if (worker_.joinable()) worker_.join();
+        if (pending_ && !error_) {
+            log_ << log_line_;
+            log_.flush();
+            std::cout << out_line_;
+        }
+    }
+    void wait() {
+        if (worker_.joinable()) worker_.join();
+        if (error_) {
+            std::exception_ptr e = error_;
+            error_ = nullptr;
+            std::rethrow_exception(e);
+        }
+        if (pending_) {
+            log_ << log_line_;
+            log_.flush();
+            std::cout << out_line_;
+            pending_ = false;
+        }
+    }
+    // st must stay untouched until the next wait()
+    void submit(const HostState& st, const Config& config, double mu_reference, fs::path path, std::string log_line,
+                std::string out_line) {
+        wait();
+        log_line_ = std::move(log_line);
+        out_line_ = std::move(out_line);
+        pending_ = true;
+        worker_ = std::thread([this, &st, &config, mu_reference, path = std::move(path)]() {
+            try {
+                write_frame(st, config, mu_reference, path);
+            } catch (...) {
+                error_ = std::current_exception();
+            }
+        });
+    }
+
+  private:
+    std::ofstream& log_;
+    std::thread worker_;
+    std::exception_ptr error_;
+    std::string log_line_, out_line_;
+    bool pending_ = false;
 };
 
 std::array<double, 3> cell_phi(const std::vector<double>& phi, size_t i) { return {phi[3 * i], phi[3 * i + 1], phi[3 * i + 2]}; }
@@ -329,23 +386,24 @@ int main(int argc, char** argv) {
         st.phi.resize(3 * cells);
         st.carbon.resize(cells);
         st.mu.resize(cells);
+        FrameWriter writer(log);
         const auto snapshot = [&]() {
             pearl_diag d{};
             gpu.check(pearl_gpu_snapshot(gpu.ctx, &d));
             const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+            writer.wait();  // the previous frame is written and st is free
             gpu.check(pearl_gpu_download(gpu.ctx, st.phi.data(), st.carbon.data(), st.mu.data(), &st.s));
             std::ostringstream fn;
             fn << "frame_" << std::setfill('0') << std::setw(6) << frames++ << ".h5";
-            write_frame(st, config, mu_reference, fs::path(output) / fn.str());
-            log << std::setprecision(17) << st.s.time << ',' << st.s.step << ',' << st.s.dt << ','
-                << d.mass / (config.nx * config.ny * config.dx * config.dy) << ',' << d.ledger << ',' << d.energy << ','
-                << d.phi_sum_error << ',' << d.c_min << ',' << d.c_max << ',' << d.mu_min << ',' << d.mu_max << ','
-                << last.cg_iterations << ',' << cg_peak << ',' << last.closure << ',' << st.s.rejected << ','
-                << st.s.shift_distance << ',' << wall << '\n';
-            log.flush();
-            std::cout << "t=" << st.s.time << " step=" << st.s.step << " dt_next=" << st.s.dt
-                      << " mass_error=" << d.ledger << " CG=" << last.cg_iterations << " rejected=" << st.s.rejected
-                      << "\n";
+            std::ostringstream line, out;
+            line << std::setprecision(17) << st.s.time << ',' << st.s.step << ',' << st.s.dt << ','
+                 << d.mass / (config.nx * config.ny * config.dx * config.dy) << ',' << d.ledger << ',' << d.energy << ','
+                 << d.phi_sum_error << ',' << d.c_min << ',' << d.c_max << ',' << d.mu_min << ',' << d.mu_max << ','
+                 << last.cg_iterations << ',' << cg_peak << ',' << last.closure << ',' << st.s.rejected << ','
+                 << st.s.shift_distance << ',' << wall << '\n';
+            out << "t=" << st.s.time << " step=" << st.s.step << " dt_next=" << st.s.dt << " mass_error=" << d.ledger
+                << " CG=" << last.cg_iterations << " rejected=" << st.s.rejected << "\n";
+            writer.submit(st, config, mu_reference, fs::path(output) / fn.str(), line.str(), out.str());
         };
         snapshot();
         bool stopped = false;
@@ -390,6 +448,7 @@ int main(int argc, char** argv) {
             }
         }
         if (S.time != saved_time) snapshot();
+        writer.wait();
         gpu.check(pearl_gpu_download(gpu.ctx, st.phi.data(), st.carbon.data(), st.mu.data(), &st.s));
         write_frame(st, config, mu_reference, fs::path(output) / "checkpoint.h5");
         std::ofstream fin(fs::path(output) / (stopped ? "STOPPED.txt" : "COMPLETED.txt"));

@@ -67,7 +67,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         # laws, initial geometry) is rounded operation by operation like it
         _run(["g++", "-O2", "-std=c++17", "-Wall", "-Wextra", "-ffp-contract=off", f"-I{INCLUDE}", f"-I{HOST}",
               *[str(HOST / n) for n in CLI_SOURCES], f"-L{BUILD}", "-lpearl_gpu", "-Wl,-rpath,$ORIGIN",
-              "-o", str(CLI)])
+              "-pthread", "-o", str(CLI)])
     return LIB
 
 
