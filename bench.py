@@ -229,9 +229,10 @@ def reference_arm(args, rank: int, world: int) -> None:
 
     ref = pyoracle.reference()
     lib, kind = (ref, "reference") if ref is not None else (pyoracle.port(), "port")
-    # Bounded: one whole warm-up step, then whole steps until --ref-seconds of
-    # timed work (about 14 s per step of the full domain on one core) or K steps.
-    warm = min(args.warmup, 1)
+    # Bounded: up to three whole warm-up steps, then whole steps until
+    # --ref-seconds of timed work (a few seconds per step of the full domain on
+    # one core) or K steps.
+    warm = min(args.warmup, 3)
     phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
     s = pyoracle.scalars_from(w.scalars)
     rc = lib.advance_n(w.params, phi, c, mu, s, warm)
@@ -246,7 +247,7 @@ def reference_arm(args, rank: int, world: int) -> None:
             raise RuntimeError(rc[1])
         timed += 1
     value = w.cells * timed / dt
-    sample = (f"{timed} timed whole steps after {warm} warm-up step of the full {w.nx}x{w.ny} workload "
+    sample = (f"{timed} timed whole steps after {warm} warm-up steps of the full {w.nx}x{w.ny} workload "
               f"(requested {args.steps}+{args.warmup}; bounded to about {args.ref_seconds:.0f} s)")
     cores = 1
     line = {
