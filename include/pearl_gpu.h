@@ -271,7 +271,9 @@ int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double
  * the simplex projection on its active set; implicit_diffusion, :1010-1093,
  * with the linear system taken as solved exactly); acceptance decisions are
  * held fixed.  On success the context holds the forward's final state; on
- * error, its initial state.  No counterpart in the reference. */
+ * error, its initial state.  Needs the FP64 step with implicit diffusion
+ * (PEARL_ERR_INVALID_ARGUMENT in mixed precision or phase-only mode).  No
+ * counterpart in the reference. */
 typedef struct pearl_adjoint_report {
     double objective;
     double grad[3]; /* dJ/dM, dJ/dsigma, dJ/dD_gamma */

@@ -146,3 +146,13 @@ def test_autograd_function_wrapper(gpu_lib):
             Js.append(_objective(w, W.perturb(w.params, rel), steps, target))
         fd = (Js[0] - Js[1]) / (2 * h)
         assert float(theta.grad[k]) == pytest.approx(fd, rel=RTOL)
+
+
+def test_adjoint_refuses_mixed_precision(gpu_lib):
+    import pearl_gpu
+
+    w = _case(nx=32, ny=32, steps=4)
+    with _ctx(w) as ctx:
+        ctx.set_precision("mixed")
+        with pytest.raises(pearl_gpu.PearlError, match="FP64"):
+            ctx.adjoint_gradient(4, 2, np.zeros((w.ny, w.nx)))
