@@ -440,6 +440,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
     cells = sum(w.cells for w in ws)
     b = pearl_gpu.Batch([(w.params, w.nx, w.ny) for w in ws], device=local,
                         group_blocks=max(args.group_blocks, 0))
+    b.set_precision(args.precision)
     pinned = []
     for i, w in enumerate(ws):
         hp = [torch.from_numpy(a).pin_memory().numpy() for a in (w.phi, w.carbon, w.mu)]
@@ -500,9 +501,11 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
             "config": {"workload": f"batched sweep: {len(ws)} instances, nx=2*spacing (spacing U{{16..96}}), "
-                                   f"ny U{{64..1024}}, f_alpha U(0.85,0.90), T_E-U(5,40)K, adaptive dt, FP64",
+                                   f"ny U{{64..1024}}, f_alpha U(0.85,0.90), T_E-U(5,40)K, adaptive dt, "
+                                   f"{args.precision}",
                        "instances": len(ws), "cells": cells, "group_blocks": st_["group_blocks"],
                        "grid_blocks": st_["grid"], "autotuned": tuned is not None,
                        "tma": None if tuned is None else tuned[1],
