@@ -175,3 +175,26 @@ def test_smallest_and_ragged_domains(gpu_lib, port, nx, ny, front):
     assert np.array_equal(trial, trial_o)
     with _ctx(w) as ctx:
         _compare_run(ctx, w, port, 8)
+
+
+def test_full_size_large_workload_replay(gpu_lib, port):
+    """The large FP64 configuration at its full size (2048x4096, 64 pairs,
+    20 K, adaptive dt): 4 accepted steps on the GPU through the run loop, then
+    the oracle replays the GPU's accepted dt sequence on the host and the
+    fields are held to the FP64 bars (about 15 s of CPU)."""
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    w = workloads.plain_large()
+    n = 4
+    with _ctx(w) as ctx:
+        infos = [ctx.advance() for _ in range(n)]
+        phi, c, mu, s = ctx.download()
+    po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    so = pyoracle.scalars_from(w.scalars)
+    rc, why, done, oinfos = port.advance_n(w.params, po, co, muo, so, n, forced_dt=[i.accepted_dt for i in infos])
+    assert rc == 0 and done == n, why
+    assert [i.cg_iterations for i in infos] == [i.cg_iterations for i in oinfos]
+    assert np.abs(phi - po).max() <= PHI_TOL
+    assert np.abs(mu - muo).max() <= MU_TOL
+    assert abs(c.sum() - co.sum()) <= MASS_RTOL * abs(co.sum())
