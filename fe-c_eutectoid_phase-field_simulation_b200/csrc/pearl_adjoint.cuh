@@ -15,30 +15,6 @@
 // Layout: every plane has the forward's pitch.  A tape slot holds the state
 // after a step (phi x3, c, mu) and that step's solution u: 6 planes.
 
-struct AdjBufs {
-    double* bphi[3];  // adjoint of phi: of the step's output on entry, of its input on exit
-    double* bc;       // adjoint of carbon
-    double* bmu;      // adjoint of mu
-    double *chi, *K, *ub, *lam, *r, *z, *p[2], *Ap, *diag;
-    double* Fb[3];  // adjoint of the propose forces
-    double* Ql[3];  // cell-local part of the phi adjoint
-};
-
-struct AdjArgs {
-    DevParams P;
-    DevBufs B;  // barrier words, status and reduction partials of the context
-    AdjBufs J;
-    int mode;            // 0: objective and adjoint seed; 1: one checkpoint segment backwards
-    const double* ckpt;  // mode 1: state at the segment start (5 planes); mode 0: final state
-    const double* tape;  // mode 1: slot j = state after step j of the segment + u_j
-    size_t slot;         // doubles per tape slot
-    const double* dts;   // accepted dt of the segment's steps
-    int len;             // steps in the segment
-    const double* target;  // mode 0: target alpha plane
-    double obs_per_sigma;  // d obs / d sigma = 16/(pi^2 eps)
-    double two_eps;        // d (2 eps sigma) / d sigma
-    double* acc;           // [0] objective, [1..3] gradient (M, sigma, D_gamma), [4] adjoint CG iterations
-};
 
 struct Cell {
     size_t i, n[4];  // centre and W, E, S, N neighbours

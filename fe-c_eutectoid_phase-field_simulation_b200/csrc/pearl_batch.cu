@@ -1,0 +1,356 @@
+// pearl_batch.cu — host side of batched instances: creation, group
+// assignment, autotuning and the batch C ABI (the kernel is pearl_batch_kernel).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pearl_host.hpp"
+
+using namespace pearl_gpu;
+
+// ============================================================ batched instances
+struct pearl_gpu_batch {
+    int device = 0, n = 0;
+    std::vector<pearl_gpu_ctx*> inst;  // host bookkeeping and buffers of every instance
+    Ctl* d_ctls = nullptr;             // the instances' control blocks, contiguous
+    Ctl* h_ctls = nullptr;             // pinned mirror
+    BatchInstance* d_inst = nullptr;
+    int* d_order = nullptr;
+    int* d_first = nullptr;
+    Ctl* d_group_ctl = nullptr;
+    double* d_group_part = nullptr;
+    int per_sm = 0, sms = 0, grid = 0, group_blocks = 0, ngroups = 0;
+    bool use_tma = true;      // TMA staging in use (needs the 32x16 tile)
+    bool tma_capable = true;  // tensor maps of every instance encoded and the shared memory granted
+    int tile_wx = 0;          // tile shape of every instance: 2^tile_wx warps side by side in x
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+    long long launches = 0;
+    std::string error;
+};
+
+namespace {
+
+int bfail(pearl_gpu_batch* b, int status, const std::string& msg) {
+    if (b) b->error = msg;
+    return status;
+}
+#define PB_CUDA(b, call)                                                                        \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return bfail(b, PEARL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Give every instance the tile shape `wx`, split the cooperative grid into
+// groups of `gb` blocks and hand out the instances longest-first to the
+// least-loaded group (cost ~ cells).  TMA staging needs the 32x16 tile.
+int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma, int wx) {
+    const int max_grid = b->per_sm * b->sms;
+    if (gb < 1 || gb > max_grid) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid group size");
+    if (wx < 0 || wx > 3) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid tile shape");
+    b->group_blocks = gb;
+    b->ngroups = max_grid / gb;
+    b->grid = b->ngroups * gb;
+    b->tile_wx = wx;
+    b->use_tma = use_tma && wx == 0 && b->tma_capable;
+    for (auto* c : b->inst) set_tile_shape(c, wx);
+    std::vector<int> idx(b->n);
+    for (int i = 0; i < b->n; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](int x, int y) {
+        return (long long)b->inst[x]->nx * b->inst[x]->ny > (long long)b->inst[y]->nx * b->inst[y]->ny;
+    });
+    std::vector<double> load(b->ngroups, 0.0);
+    std::vector<std::vector<int>> lists(b->ngroups);
+    for (int i : idx) {
+        // a group's blocks share an instance's tiles: cost = cells / min(blocks, tiles)
+        const pearl_gpu_ctx* c = b->inst[i];
+        const double cells = (double)c->nx * c->ny;
+        const double cost = cells / std::max(1, std::min(gb, c->P.ntiles));
+        int best = 0;
+        for (int g = 1; g < b->ngroups; ++g)
+            if (load[g] < load[best]) best = g;
+        load[best] += cost;
+        lists[best].push_back(i);
+    }
+    std::vector<int> order, first(1, 0);
+    for (int g = 0; g < b->ngroups; ++g) {
+        order.insert(order.end(), lists[g].begin(), lists[g].end());
+        first.push_back((int)order.size());
+    }
+    cudaFree(b->d_order);
+    cudaFree(b->d_first);
+    cudaFree(b->d_group_ctl);
+    cudaFree(b->d_group_part);
+    b->d_order = nullptr;
+    b->d_first = nullptr;
+    b->d_group_ctl = nullptr;
+    b->d_group_part = nullptr;
+    PB_CUDA(b, cudaMalloc(&b->d_order, sizeof(int) * std::max(1, b->n)));
+    PB_CUDA(b, cudaMalloc(&b->d_first, sizeof(int) * first.size()));
+    PB_CUDA(b, cudaMalloc(&b->d_group_ctl, sizeof(Ctl) * b->ngroups));
+    PB_CUDA(b, cudaMalloc(&b->d_group_part, sizeof(double) * (size_t)b->ngroups * 2 * gb * kMaxRed));
+    PB_CUDA(b, cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+    PB_CUDA(b, cudaMemcpy(b->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+    PB_CUDA(b, cudaMemset(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups));
+    // per-instance descriptors (tensor maps, parameters, buffers)
+    std::vector<BatchInstance> hi(b->n);
+    for (int i = 0; i < b->n; ++i) {
+        std::memcpy(hi[i].maps, b->inst[i]->maps, sizeof hi[i].maps);
+        hi[i].P = b->inst[i]->P;
+        hi[i].B = b->inst[i]->B;
+    }
+    PB_CUDA(b, cudaMemcpy(b->d_inst, hi.data(), sizeof(BatchInstance) * b->n, cudaMemcpyHostToDevice));
+    return PEARL_OK;
+}
+
+int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
+    PB_CUDA(b, cudaSetDevice(b->device));
+    PB_CUDA(b, cudaMemsetAsync(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups, b->stream));
+    BatchArgs args{};
+    args.inst = b->d_inst;
+    args.order = b->d_order;
+    args.first = b->d_first;
+    args.group_blocks = b->group_blocks;
+    args.group_ctl = b->d_group_ctl;
+    args.group_part = b->d_group_part;
+    args.use_tma = b->use_tma ? 1 : 0;
+    args.L = L;
+    void* kargs[] = {&args};
+    PB_CUDA(b, cudaEventRecord(b->ev0, b->stream));
+    PB_CUDA(b, cudaLaunchCooperativeKernel((const void*)pearl_batch_kernel, dim3(b->grid), dim3(kThreads), kargs,
+                                           b->use_tma ? kTmaSmemBytes : 0, b->stream));
+    b->launches++;
+    PB_CUDA(b, cudaEventRecord(b->ev1, b->stream));
+    PB_CUDA(b, cudaMemcpyAsync(b->h_ctls, b->d_ctls, sizeof(Ctl) * b->n, cudaMemcpyDeviceToHost, b->stream));
+    PB_CUDA(b, cudaStreamSynchronize(b->stream));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    b->last_ms = ms;
+    for (int i = 0; i < b->n; ++i) *b->inst[i]->h_ctl = b->h_ctls[i];
+    return PEARL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pearl_gpu_batch_destroy(pearl_gpu_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto* c : b->inst) {
+        if (c) c->d_ctl = nullptr;  // owned by the batch
+        pearl_gpu_destroy(c);
+    }
+    cudaFree(b->d_ctls);
+    if (b->h_ctls) cudaFreeHost(b->h_ctls);
+    cudaFree(b->d_inst);
+    cudaFree(b->d_order);
+    cudaFree(b->d_first);
+    cudaFree(b->d_group_ctl);
+    cudaFree(b->d_group_part);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    delete b;
+}
+
+int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, const int* ny, int device,
+                           int group_blocks, pearl_gpu_batch** out) {
+    if (!out || n < 1 || !params || !nx || !ny) return PEARL_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    pearl_gpu_batch* b = new pearl_gpu_batch();
+    b->device = device;
+    b->n = n;
+    auto bail = [&](int rc) {
+        pearl_gpu_batch_destroy(b);
+        return rc;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(PEARL_ERR_NO_DEVICE);
+    b->inst.assign(n, nullptr);
+    if (cudaMalloc(&b->d_ctls, sizeof(Ctl) * n) != cudaSuccess ||
+        cudaMallocHost(&b->h_ctls, sizeof(Ctl) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_inst, sizeof(BatchInstance) * n) != cudaSuccess)
+        return bail(PEARL_ERR_CUDA);
+    std::memset(b->h_ctls, 0, sizeof(Ctl) * n);
+    bool tma = true;
+    for (int i = 0; i < n; ++i) {
+        const int rc = pearl_gpu_create(&params[i], nx[i], ny[i], device, &b->inst[i]);
+        if (rc) return bail(rc);
+        pearl_gpu_ctx* c = b->inst[i];
+        cudaFree(c->d_ctl);  // the batch keeps every control block in one array
+        c->d_ctl = b->d_ctls + i;
+        c->B.ctl = c->d_ctl;
+        if (cudaMemcpy(c->d_ctl, c->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(PEARL_ERR_CUDA);
+        tma = tma && c->use_tma;
+    }
+    if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return bail(PEARL_ERR_CUDA);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+    if (tma &&
+        cudaFuncSetAttribute(pearl_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
+            cudaSuccess)
+        tma = false;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->per_sm, pearl_batch_kernel, kThreads,
+                                                      tma ? kTmaSmemBytes : 0) != cudaSuccess ||
+        b->per_sm < 1)
+        return bail(PEARL_ERR_CUDA);
+    b->tma_capable = tma;
+    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : 4, tma, 0);
+    if (rc) return bail(rc);
+    *out = b;
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_upload(pearl_gpu_batch* b, int i, const double* phi, const double* carbon, const double* mu,
+                           const pearl_scalars* scalars) {
+    if (!b || i < 0 || i >= b->n) return PEARL_ERR_INVALID_ARGUMENT;
+    const int rc = pearl_gpu_upload(b->inst[i], phi, carbon, mu, scalars);
+    if (rc) return bfail(b, rc, pearl_gpu_last_error(b->inst[i]));
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_download(pearl_gpu_batch* b, int i, double* phi, double* carbon, double* mu,
+                             pearl_scalars* scalars) {
+    if (!b || i < 0 || i >= b->n) return PEARL_ERR_INVALID_ARGUMENT;
+    const int rc = pearl_gpu_download(b->inst[i], phi, carbon, mu, scalars);
+    if (rc) return bfail(b, rc, pearl_gpu_last_error(b->inst[i]));
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_run(pearl_gpu_batch* b, const pearl_run_limits* limits, pearl_run_report* reports,
+                        int* status) {
+    if (!b || !limits || limits->max_steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
+    int rc = batch_launch(b, *limits);
+    if (rc) return rc;
+    int first_bad = PEARL_OK;
+    for (int i = 0; i < b->n; ++i) {
+        const Ctl& h = b->h_ctls[i];
+        if (reports) {
+            reports[i].steps = h.steps;
+            reports[i].cg_total = h.cg_total;
+            reports[i].cg_peak = h.cg_peak;
+            reports[i].reached_stop = h.reached_stop;
+            reports[i].last = h.last;
+        }
+        if (status) status[i] = h.status;
+        if (h.status == PEARL_ERR_DEVICE_WAIT) first_bad = PEARL_ERR_DEVICE_WAIT;
+    }
+    if (first_bad) return bfail(b, first_bad, "device grid barrier wait exceeded its limit");
+    return PEARL_OK;
+}
+
+int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, int* use_tma, int* tile_warps_x) {
+    if (!b || steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
+    PB_CUDA(b, cudaSetDevice(b->device));
+    // back up every instance's current state (5 planes) and control block
+    std::vector<double*> backup(b->n, nullptr);
+    auto release = [&]() {
+        for (double* p : backup) cudaFree(p);
+    };
+    for (int i = 0; i < b->n; ++i) {
+        pearl_gpu_ctx* c = b->inst[i];
+        const size_t bytes = 5 * plane_elems(c) * sizeof(double);
+        if (cudaMalloc(&backup[i], bytes) != cudaSuccess) {
+            release();
+            return bfail(b, PEARL_ERR_CUDA, "autotune backup allocation");
+        }
+        cudaMemcpyAsync(backup[i], c->B.phi[c->h_ctl->cur][0], bytes, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    // the instances' host control blocks are authoritative (uploads update them)
+    std::vector<Ctl> saved(b->n);
+    for (int i = 0; i < b->n; ++i) saved[i] = *b->inst[i]->h_ctl;
+    double best_ms = 1e300;
+    int best_gb = b->group_blocks, best_wx = b->tile_wx;
+    bool best_tma = b->use_tma;
+    const int cands[] = {1, 2, 4, 8, 16};
+    pearl_run_limits L{1, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
+    // tile shapes 32x16 (with and without TMA staging), 64x8 and 128x4
+    struct Shape {
+        int wx;
+        bool tma;
+    };
+    std::vector<Shape> shapes;
+    if (b->tma_capable) shapes.push_back({0, true});
+    shapes.push_back({0, false});
+    shapes.push_back({1, false});
+    shapes.push_back({2, false});
+    for (const Shape& sh : shapes) {
+        const int tma = sh.tma ? 1 : 0;
+        for (int gb : cands) {
+            if (gb > b->per_sm * b->sms) continue;
+            int rc = batch_configure(b, gb, tma != 0, sh.wx);
+            double ms = 0;
+            for (int s = 0; rc == PEARL_OK && s < steps; ++s) {
+                rc = batch_launch(b, L);
+                ms += b->last_ms;
+            }
+            // restore
+            for (int i = 0; i < b->n; ++i) {
+                pearl_gpu_ctx* c = b->inst[i];
+                cudaMemcpyAsync(c->B.phi[saved[i].cur][0], backup[i], 5 * plane_elems(c) * sizeof(double),
+                                cudaMemcpyDeviceToDevice, b->stream);
+            }
+            std::memcpy(b->h_ctls, saved.data(), sizeof(Ctl) * b->n);
+            cudaMemcpyAsync(b->d_ctls, b->h_ctls, sizeof(Ctl) * b->n, cudaMemcpyHostToDevice, b->stream);
+            cudaStreamSynchronize(b->stream);
+            for (int i = 0; i < b->n; ++i) *b->inst[i]->h_ctl = saved[i];
+            if (rc) {
+                release();
+                return rc;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_gb = gb;
+                best_tma = tma != 0;
+                best_wx = sh.wx;
+            }
+        }
+    }
+    release();
+    const int rc = batch_configure(b, best_gb, best_tma, best_wx);
+    if (group_blocks) *group_blocks = best_gb;
+    if (use_tma) *use_tma = best_tma ? 1 : 0;
+    if (tile_warps_x) *tile_warps_x = 1 << best_wx;
+    return rc;
+}
+
+int pearl_gpu_batch_configure(pearl_gpu_batch* b, int group_blocks, int use_tma, int tile_warps_x) {
+    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
+    const int wx = tile_warps_x == 1 ? 0 : tile_warps_x == 2 ? 1 : tile_warps_x == 4 ? 2 : tile_warps_x == 8 ? 3 : -1;
+    if (wx < 0) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "tile_warps_x must be 1, 2, 4 or 8");
+    PB_CUDA(b, cudaSetDevice(b->device));
+    return batch_configure(b, group_blocks, use_tma != 0, wx);
+}
+
+int pearl_gpu_batch_set_precision(pearl_gpu_batch* b, int precision) {
+    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
+    for (auto* c : b->inst) {
+        const int rc = pearl_gpu_set_precision(c, precision);
+        if (rc) return bfail(b, rc, "invalid precision");
+    }
+    return batch_configure(b, b->group_blocks, b->use_tma, b->tile_wx);
+}
+
+int pearl_gpu_batch_stats(const pearl_gpu_batch* b, long long* launches, int* grid_blocks, int* group_blocks,
+                          double* last_kernel_ms) {
+    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
+    if (launches) *launches = b->launches;
+    if (grid_blocks) *grid_blocks = b->grid;
+    if (group_blocks) *group_blocks = b->group_blocks;
+    if (last_kernel_ms) *last_kernel_ms = b->last_ms;
+    return PEARL_OK;
+}
+
+const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* b) { return b ? b->error.c_str() : "null batch"; }
+
+}  // extern "C"
+

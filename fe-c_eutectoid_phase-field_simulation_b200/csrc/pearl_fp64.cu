@@ -32,46 +32,11 @@
 
 #include <cudaTypedefs.h>
 
-#include "pearl_device.cuh"
-#include "pearl_gpu.h"
+#include "pearl_kernels.cuh"
 
 namespace pearl_gpu {
 
-enum Mode : int {
-    kModeRun = 0,
-    kModePropose = 1,
-    kModeMix = 2,
-    kModeDiffusion = 3,
-    kModeEnergy = 4,
-    kModeValid = 5,
-    kModeSnapshot = 6,
-    kModeMaybeShift = 7,
-    kModeSmooth = 8,
-    kModeMixSums = 9,
-    kModeInitComposition = 10,
-};
 
-struct KArgs {
-    CUtensorMap maps[kMapCount];  // 2-D TMA descriptors of the staged planes (valid when use_tma)
-    int use_tma;
-    DevParams P;
-    DevBufs B;
-    int mode;
-    double dt;  // diagnostic modes
-    pearl_run_limits L;
-    double shift_trigger, shift_target, shift_c_gamma;
-    int smooth_max_steps, smooth_min_steps;
-    double smooth_energy_rtol, smooth_max_phase_change;
-    double init_mu;
-    // run-mode recording for the adjoint (all may be null): forced accepted-dt
-    // sequence, log of accepted dt, and a tape slot per accepted step holding
-    // the new state (phi x3, c, mu) and the diffusion solution u, tape_slot
-    // doubles apart.
-    const double* forced_dt;
-    double* dt_log;
-    double* tape;
-    size_t tape_slot;
-};
 
 // One domain as seen by one block: its parameters, buffers and tensor maps,
 // the block's index in the group of blocks that shares the domain, the
@@ -1728,22 +1693,6 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
 // into groups of `group_blocks` blocks; each group runs the same `advance`
 // device code on its own list of instances, one after another, with barriers
 // and reductions local to the group.
-struct alignas(64) BatchInstance {
-    CUtensorMap maps[kMapCount];
-    DevParams P;
-    DevBufs B;  // B.ctl: the instance's control block; B.part: unused
-};
-
-struct BatchArgs {
-    const BatchInstance* inst;
-    const int* order;  // instance ids grouped by block group
-    const int* first;  // group g owns order[first[g] .. first[g+1])
-    int group_blocks;
-    Ctl* group_ctl;      // [groups] barrier words and error status
-    double* group_part;  // [groups][2][group_blocks][kMaxRed]
-    int use_tma;
-    pearl_run_limits L;
-};
 
 __global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
     const int g = blockIdx.x / args.group_blocks, bid = blockIdx.x % args.group_blocks;
@@ -1855,1479 +1804,3 @@ __global__ void wait_limit_selftest_kernel(Ctl* ctl) { grid_barrier(ctl, gridDim
 
 }  // namespace pearl_gpu
 
-// ====================================================================== host side
-using namespace pearl_gpu;
-
-struct pearl_gpu_ctx {
-    CUtensorMap maps[kMapCount];
-    bool use_tma = false;
-    int device = 0;
-    int nx = 0, ny = 0, pitch = 0;
-    cudaStream_t stream = nullptr;
-    pearl_params params{};
-    DevParams P{};
-    DevBufs B{};
-    double* slab = nullptr;
-    Ctl* d_ctl = nullptr;
-    Ctl* h_ctl = nullptr;  // pinned
-    double* d_stage = nullptr;  // dense device staging of one host state (5 n doubles)
-    size_t stage_elems = 0;
-    int grid = 0;
-    long long launches = 0;
-    double last_ms = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int adj_grid = 0;  // cooperative grid of the adjoint kernel (0 until first use)
-    std::string error;
-};
-
-namespace {
-
-constexpr int kDefaultWarpsXLog2 = 0;
-
-const char* why_text(int why) {
-    switch (why) {
-        case PEARL_WHY_PHASE_INCREMENT: return "phase increment";
-        case PEARL_WHY_LINEAR_CLOSURE: return "linear/closure";
-        case PEARL_WHY_BOUNDS: return "composition/phase bounds";
-        case PEARL_WHY_MASS: return "mass conservation";
-        case PEARL_WHY_ENERGY: return "free-energy increase";
-        default: return "";
-    }
-}
-
-int fail(pearl_gpu_ctx* ctx, int status, const std::string& msg) {
-    if (ctx) ctx->error = msg;
-    return status;
-}
-
-int cuda_fail(pearl_gpu_ctx* ctx, cudaError_t e, const char* what) {
-    return fail(ctx, PEARL_ERR_CUDA, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
-}
-
-#define PG_CUDA(ctx, call)                                  \
-    do {                                                    \
-        cudaError_t e_ = (call);                            \
-        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
-    } while (0)
-
-bool valid_params(const pearl_params* p) {
-    for (int i = 0; i < 3; ++i) {
-        // Parabola::validate (pearl_serial.cpp:76-79)
-        if (!std::isfinite(p->A[i]) || !std::isfinite(p->B[i]) || !std::isfinite(p->C[i]) || !std::isfinite(p->D[i]) ||
-            p->A[i] <= 0.0 || p->D[i] < 0.0)
-            return false;
-        if (!(p->tau[i] > 0) || !std::isfinite(p->tau[i])) return false;
-    }
-    // InterfaceParameters::validate / PhaseParameters::validate (:414-419, :522-529)
-    if (!(p->epsilon > 0) || !(p->sigma > 0) || p->triple < 0 || !std::isfinite(p->epsilon) ||
-        !std::isfinite(p->sigma) || !std::isfinite(p->triple))
-        return false;
-    if (!(p->Vm > 0) || !std::isfinite(p->Vm)) return false;
-    if (!(p->dx > 0) || !(p->dy > 0) || !std::isfinite(p->dx + p->dy)) return false;
-    if (p->cg_max < 0 || p->max_retries < 0) return false;
-    return true;
-}
-
-double host_psi(const pearl_params* p, int a, double mu) {
-    const double d = mu - p->B[a];
-    return std::fma(-0.25 / p->A[a], d * d, p->C[a]);
-}
-
-// Tile of (32 << wx) x (2 << (3 - wx)) cells: 2^wx warps side by side in x.
-void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2) {
-    DevParams& P = ctx->P;
-    P.warps_x_log2 = wx_log2;
-    const int tile_w = 32 << wx_log2, tile_h = 2 << (3 - wx_log2);
-    P.ntx = (ctx->nx + tile_w - 1) / tile_w;
-    P.nty = (ctx->ny + tile_h - 1) / tile_h;
-    P.ntiles = P.ntx * P.nty;
-}
-
-void fill_dev_params(pearl_gpu_ctx* ctx) {
-    const pearl_params* p = &ctx->params;
-    DevParams& P = ctx->P;
-    P.nx = ctx->nx;
-    P.ny = ctx->ny;
-    P.pitch = ctx->pitch;
-    // Tile shape: warps side by side in x give longer contiguous row segments
-    // (better DRAM locality); PEARL_GPU_TILE_WARPS_X = 1, 2, 4 or 8 overrides.
-    int wx_log2 = kDefaultWarpsXLog2;
-    if (const char* e = std::getenv("PEARL_GPU_TILE_WARPS_X")) {
-        const int w = std::atoi(e);
-        wx_log2 = w >= 8 ? 3 : w >= 4 ? 2 : w >= 2 ? 1 : 0;
-    }
-    set_tile_shape(ctx, wx_log2);
-    P.dx = p->dx;
-    P.dy = p->dy;
-    P.dx2 = p->dx * p->dx;
-    P.dy2 = p->dy * p->dy;
-    P.Vm = p->Vm;
-    P.eps = p->epsilon;
-    const double pi = std::acos(-1.);
-    P.obs = 16 * p->sigma / (pi * pi * p->epsilon);
-    P.tr = p->triple / p->epsilon;
-    P.two_eps_sigma = 2 * p->epsilon * p->sigma;
-    P.eps_sigma = p->epsilon * p->sigma;
-    double tmin = p->tau[0];
-    for (int i = 0; i < 3; ++i) {
-        P.tau[i] = p->tau[i];
-        if (p->tau[i] < tmin) tmin = p->tau[i];
-        P.A[i] = p->A[i];
-        P.B[i] = p->B[i];
-        P.C[i] = p->C[i];
-        P.D[i] = p->D[i];
-        P.chi_p[i] = 1.0 / (2.0 * p->A[i]);
-        P.neg_q_A[i] = -0.25 / p->A[i];
-        P.two_A[i] = 2.0 * p->A[i];
-    }
-    P.tau_min = tmin;
-    P.mu_ref = p->mu_reference;
-    // mixed-precision constants (P.mixed itself is set by pearl_gpu_set_precision)
-    P.m_obs = (float)P.obs;
-    P.m_tr = (float)P.tr;
-    P.m_kx = (float)(P.two_eps_sigma / P.dx2);
-    P.m_ky = (float)(P.two_eps_sigma / P.dy2);
-    P.m_rVm = (float)(1.0 / p->Vm);
-    for (int b = 0; b < 2; ++b) {
-        const double mr = p->mu_reference;
-        P.m_pa[b] = (float)(host_psi(p, b, mr) - host_psi(p, 2, mr));
-        P.m_pb[b] = (float)(-(mr - p->B[b]) / (2.0 * p->A[b]) + (mr - p->B[2]) / (2.0 * p->A[2]));
-        P.m_pc[b] = (float)(-0.25 / p->A[b] + 0.25 / p->A[2]);
-    }
-    for (int i = 0; i < 3; ++i) P.m_tau[i] = (float)p->tau[i];
-    P.m_tau_min = (float)tmin;
-    P.psi_t[0] = host_psi(p, 0, p->mu_reference) - host_psi(p, 2, p->mu_reference);
-    P.psi_t[1] = host_psi(p, 1, p->mu_reference) - host_psi(p, 2, p->mu_reference);
-    P.psi_t[2] = 0;
-    P.dt_max = p->dt_max;
-    P.dt_min = p->dt_min;
-    P.max_phase_change = p->max_phase_change;
-    P.cg_rtol = p->cg_rtol;
-    P.cg_atol = p->cg_atol;
-    P.closure_tol = p->closure_tol;
-    P.energy_rtol = p->energy_rtol;
-    P.energy_atol = p->energy_atol;
-    const int gxgy = ctx->nx * ctx->ny;
-    P.mass_scale = gxgy * p->dx * p->dy * 1e-6;
-    P.energy_scale = p->sigma * std::max(ctx->nx * p->dx, ctx->ny * p->dy);
-    P.cg_max = p->cg_max;
-    P.max_retries = p->max_retries;
-    P.check_energy = p->check_energy;
-    P.phase_only = p->phase_only;
-    // reciprocals of the constant divisors (RN(1/b), host IEEE division)
-    P.r_Vm = 1.0 / P.Vm;
-    P.r_dx = 1.0 / P.dx;
-    P.r_dy = 1.0 / P.dy;
-    P.r_dx2 = 1.0 / P.dx2;
-    P.r_dy2 = 1.0 / P.dy2;
-    P.r_3 = 1.0 / 3.0;
-    for (int i = 0; i < 3; ++i) P.r_two_A[i] = 1.0 / P.two_A[i];
-    const double divisors[] = {P.Vm, P.dx, P.dy, P.dx2, P.dy2, 3.0, P.two_A[0], P.two_A[1], P.two_A[2]};
-    const double recips[] = {P.r_Vm, P.r_dx, P.r_dy, P.r_dx2, P.r_dy2, P.r_3, P.r_two_A[0], P.r_two_A[1], P.r_two_A[2]};
-    P.exact_div = 1;
-    for (int i = 0; i < 9; ++i)
-        if (std::fpclassify(divisors[i]) != FP_NORMAL || std::fpclassify(recips[i]) != FP_NORMAL) P.exact_div = 0;
-}
-
-int pull_ctl(pearl_gpu_ctx* ctx) {
-    PG_CUDA(ctx, cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return PEARL_OK;
-}
-
-int push_ctl(pearl_gpu_ctx* ctx) {
-    PG_CUDA(ctx, cudaMemcpyAsync(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice, ctx->stream));
-    return PEARL_OK;
-}
-
-// Launch the persistent kernel in `mode`; on return h_ctl holds the device
-// control block.  Maps the device status to the reference's messages.
-int launch(pearl_gpu_ctx* ctx, KArgs& args) {
-    PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    ctx->h_ctl->status = 0;
-    ctx->h_ctl->why = 0;
-    ctx->h_ctl->bar_count = 0;
-    int rc = push_ctl(ctx);
-    if (rc) return rc;
-    args.P = ctx->P;
-    args.B = ctx->B;
-    void* kargs[] = {&args};
-    PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    args.use_tma = ctx->use_tma ? 1 : 0;
-    if (ctx->use_tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(ctx->grid), dim3(kThreads), kargs,
-                                             ctx->use_tma ? kTmaSmemBytes : 0,
-                                             ctx->stream));
-    ctx->launches++;
-    PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-    rc = pull_ctl(ctx);
-    if (rc) return rc;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    ctx->last_ms = ms;
-    const int st = ctx->h_ctl->status;
-    if (st == PEARL_OK) return PEARL_OK;
-    ctx->h_ctl->energy_valid = 0;
-    switch (st) {
-        case PEARL_ERR_INVALID_ADVANCE_TIME: return fail(ctx, st, "invalid advance time");
-        case PEARL_ERR_REJECTED_BELOW_DT_MIN:
-            return fail(ctx, st, std::string("step rejected below dt_min: ") + why_text(ctx->h_ctl->why));
-        case PEARL_ERR_RETRY_LIMIT: return fail(ctx, st, std::string("step retry limit: ") + why_text(ctx->h_ctl->why));
-        case PEARL_ERR_MIXTURE: return fail(ctx, st, "Invalid mixture coefficients");
-        case PEARL_ERR_SIMPLEX: return fail(ctx, st, "Simplex projection failed");
-        case PEARL_ERR_MAX_STEPS: return fail(ctx, st, "configured max_steps reached before end_time");
-        case PEARL_ERR_UNSAFE_SHIFT: return fail(ctx, st, "unsafe shift: removed strip contains gamma");
-        case PEARL_ERR_NONFINITE_CARBON: return fail(ctx, st, "Nonfinite total carbon");
-        case PEARL_ERR_SMOOTHING:
-            return fail(ctx, st, ctx->h_ctl->why == 1 ? "nonfinite smoothing force"
-                                                      : "sharp smoothing could not find an energy-decreasing step");
-        case PEARL_ERR_DEVICE_WAIT:
-            // a grid barrier gave up waiting: reset the barrier words before any further launch
-            ctx->h_ctl->bar_count = 0;
-            push_ctl(ctx);
-            return fail(ctx, st, "device grid barrier wait exceeded its limit");
-        default: return fail(ctx, st, "invalid argument");
-    }
-}
-
-size_t plane_elems(const pearl_gpu_ctx* ctx) { return (size_t)ctx->pitch * ctx->ny; }
-
-// 2-D TMA descriptors for the planes the stencil phases stage through shared
-// memory: box (kBoxW x kBoxH) float64, dims (nx, ny), row stride pitch*8 bytes,
-// zero fill outside.  Returns false when the driver cannot encode them; the
-// kernels then read the planes directly.
-bool build_tensor_maps(pearl_gpu_ctx* ctx) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        cudaDriverEntryPointQueryResult q;
-        void* fn = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn)
-            return false;
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
-    const DevBufs& B = ctx->B;
-    double* planes[kMapCount] = {};
-    for (int s = 0; s < 2; ++s) {
-        for (int a = 0; a < 3; ++a) planes[kMapState + 5 * s + a] = B.phi[s][a];
-        planes[kMapState + 5 * s + 3] = B.c[s];
-        planes[kMapState + 5 * s + 4] = B.mu[s];
-    }
-    planes[kMapK] = B.K;
-    planes[kMapChi] = B.chi;
-    planes[kMapIcpt] = B.icpt;
-    planes[kMapX] = B.x;
-    planes[kMapZ] = B.z;
-    planes[kMapP0] = B.p[0];
-    planes[kMapP1] = B.p[1];
-    planes[kMapWE] = B.wE;
-    planes[kMapWN] = B.wN;
-    planes[kMapR] = B.r;
-    planes[kMapAp] = B.Ap;
-    planes[kMapDiag] = B.diag;
-    for (int m = 0; m < kMapCount; ++m) {
-        const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
-        const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(double)};
-        const cuuint32_t box[2] = {(cuuint32_t)kBoxW, (cuuint32_t)kBoxH};
-        const cuuint32_t estr[2] = {1, 1};
-        if (encode(&ctx->maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, planes[m], dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-            return false;
-    }
-    return true;
-}
-
-int ensure_stage(pearl_gpu_ctx* ctx) {
-    if (!ctx->d_stage) PG_CUDA(ctx, cudaMalloc(&ctx->d_stage, ctx->stage_elems * sizeof(double)));
-    return PEARL_OK;
-}
-
-// Host fields in the reference's gathered layout (phi (y,x,a) interleaved,
-// carbon and mu dense) travel as they are into a dense device staging buffer
-// [phi 3n | carbon n | mu n]; these kernels move them to and from the padded
-// SoA planes of one state set, so the host does no per-element work.
-__global__ void unpack_state_kernel(const double* __restrict__ st, long long n, int nx, int pitch,
-                                    double* p0, double* p1, double* p2, double* c, double* mu) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const long long y = i / nx, x = i - y * nx;
-        const size_t d = (size_t)y * pitch + x;
-        if (p0) {
-            p0[d] = st[3 * i];
-            p1[d] = st[3 * i + 1];
-            p2[d] = st[3 * i + 2];
-        }
-        if (c) c[d] = st[3 * n + i];
-        if (mu) mu[d] = st[4 * n + i];
-    }
-}
-
-__global__ void pack_state_kernel(double* __restrict__ st, long long n, int nx, int pitch, const double* p0,
-                                  const double* p1, const double* p2, const double* c, const double* mu) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const long long y = i / nx, x = i - y * nx;
-        const size_t d = (size_t)y * pitch + x;
-        if (p0) {
-            st[3 * i] = p0[d];
-            st[3 * i + 1] = p1[d];
-            st[3 * i + 2] = p2[d];
-        }
-        if (c) st[3 * n + i] = c[d];
-        if (mu) st[4 * n + i] = mu[d];
-    }
-}
-
-int stage_grid(const pearl_gpu_ctx* ctx) {
-    const long long n = (long long)ctx->nx * ctx->ny;
-    return (int)std::max(1LL, std::min<long long>((n + 255) / 256, 148LL * 16));
-}
-
-int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* carbon, const double* mu) {
-    if (int rc = ensure_stage(ctx)) return rc;
-    const size_t n = (size_t)ctx->nx * ctx->ny;
-    double* st = ctx->d_stage;
-    if (phi) PG_CUDA(ctx, cudaMemcpyAsync(st, phi, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if (carbon)
-        PG_CUDA(ctx, cudaMemcpyAsync(st + 3 * n, carbon, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if (mu) PG_CUDA(ctx, cudaMemcpyAsync(st + 4 * n, mu, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    unpack_state_kernel<<<stage_grid(ctx), 256, 0, ctx->stream>>>(
-        st, (long long)n, ctx->nx, ctx->pitch, phi ? ctx->B.phi[set][0] : nullptr, ctx->B.phi[set][1],
-        ctx->B.phi[set][2], carbon ? ctx->B.c[set] : nullptr, mu ? ctx->B.mu[set] : nullptr);
-    ctx->launches++;
-    PG_CUDA(ctx, cudaGetLastError());
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return PEARL_OK;
-}
-
-int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, double* mu) {
-    if (int rc = ensure_stage(ctx)) return rc;
-    const size_t n = (size_t)ctx->nx * ctx->ny;
-    double* st = ctx->d_stage;
-    pack_state_kernel<<<stage_grid(ctx), 256, 0, ctx->stream>>>(
-        st, (long long)n, ctx->nx, ctx->pitch, phi ? ctx->B.phi[set][0] : nullptr, ctx->B.phi[set][1],
-        ctx->B.phi[set][2], carbon ? ctx->B.c[set] : nullptr, mu ? ctx->B.mu[set] : nullptr);
-    ctx->launches++;
-    PG_CUDA(ctx, cudaGetLastError());
-    if (phi) PG_CUDA(ctx, cudaMemcpyAsync(phi, st, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    if (carbon)
-        PG_CUDA(ctx, cudaMemcpyAsync(carbon, st + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    if (mu) PG_CUDA(ctx, cudaMemcpyAsync(mu, st + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return PEARL_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-const char* pearl_gpu_status_string(int status) {
-    switch (status) {
-        case PEARL_OK: return "ok";
-        case PEARL_ERR_INVALID_ARGUMENT: return "invalid argument";
-        case PEARL_ERR_CUDA: return "CUDA error";
-        case PEARL_ERR_INVALID_ADVANCE_TIME: return "invalid advance time";
-        case PEARL_ERR_REJECTED_BELOW_DT_MIN: return "step rejected below dt_min";
-        case PEARL_ERR_RETRY_LIMIT: return "step retry limit";
-        case PEARL_ERR_MIXTURE: return "Invalid mixture coefficients";
-        case PEARL_ERR_SIMPLEX: return "Simplex projection failed";
-        case PEARL_ERR_MAX_STEPS: return "configured max_steps reached before end_time";
-        case PEARL_ERR_DEVICE_WAIT: return "device wait limit exceeded";
-        case PEARL_ERR_UNSAFE_SHIFT: return "unsafe shift: removed strip contains gamma";
-        case PEARL_ERR_NONFINITE_CARBON: return "Nonfinite total carbon";
-        case PEARL_ERR_NO_DEVICE: return "no CUDA device";
-        case PEARL_ERR_TOO_LARGE: return "domain exceeds the no-allocation scratch limit of 262144 cells";
-        case PEARL_ERR_SMOOTHING: return "sharp smoothing failed";
-        default: return "unknown status";
-    }
-}
-
-const char* pearl_gpu_last_error(const pearl_gpu_ctx* ctx) { return ctx ? ctx->error.c_str() : "null context"; }
-
-int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pearl_gpu_ctx** out) {
-    if (!out) return PEARL_ERR_INVALID_ARGUMENT;
-    *out = nullptr;
-    if (!params || nx < 3 || ny < 2 || !valid_params(params)) return PEARL_ERR_INVALID_ARGUMENT;
-    if ((long long)nx * ny > 2000000000LL) return PEARL_ERR_INVALID_ARGUMENT;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return PEARL_ERR_NO_DEVICE;
-    pearl_gpu_ctx* ctx = new pearl_gpu_ctx();
-    ctx->device = device;
-    ctx->nx = nx;
-    ctx->ny = ny;
-    ctx->pitch = (nx + 31) / 32 * 32;
-    ctx->params = *params;
-    auto bail = [&](int rc) {
-        pearl_gpu_destroy(ctx);
-        return rc;
-    };
-    if (cudaSetDevice(device) != cudaSuccess) return bail(PEARL_ERR_CUDA);
-    int coop = 0, sms = 0;
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (!coop) return bail(PEARL_ERR_NO_DEVICE);
-    fill_dev_params(ctx);
-    // TMA staging of the stencil phases needs the 32x16 tile; PEARL_GPU_TMA=0 turns it off.
-    const char* tma_env = std::getenv("PEARL_GPU_TMA");
-    ctx->use_tma = ctx->P.warps_x_log2 == 0 && !(tma_env && std::atoi(tma_env) == 0);
-    if (ctx->use_tma &&
-        cudaFuncSetAttribute(pearl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
-            cudaSuccess)
-        ctx->use_tma = false;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads,
-                                                      ctx->use_tma ? kTmaSmemBytes : 0) != cudaSuccess ||
-        per_sm < 1)
-        return bail(PEARL_ERR_CUDA);
-    ctx->grid = std::max(1, std::min(per_sm * sms, ctx->P.ntiles));
-    // state: 2 x (3 phi + c + mu); work: K chi icpt diag x r z p0 p1 Ap  -> 20 planes
-    const size_t pe = plane_elems(ctx);
-    const int nplanes = 22;
-    const size_t part = (size_t)2 * ctx->grid * kMaxRed;
-    if (cudaMalloc(&ctx->slab, (nplanes * pe + part) * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
-    if (cudaMemset(ctx->slab, 0, (nplanes * pe + part) * sizeof(double)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
-    double* q = ctx->slab;
-    for (int s = 0; s < 2; ++s) {
-        for (int a = 0; a < 3; ++a, q += pe) ctx->B.phi[s][a] = q;
-        ctx->B.c[s] = q;
-        q += pe;
-        ctx->B.mu[s] = q;
-        q += pe;
-    }
-    ctx->B.K = q; q += pe;
-    ctx->B.chi = q; q += pe;
-    ctx->B.icpt = q; q += pe;
-    ctx->B.diag = q; q += pe;
-    ctx->B.x = q; q += pe;
-    ctx->B.r = q; q += pe;
-    ctx->B.z = q; q += pe;
-    ctx->B.p[0] = q; q += pe;
-    ctx->B.p[1] = q; q += pe;
-    ctx->B.Ap = q; q += pe;
-    ctx->B.wE = q; q += pe;
-    ctx->B.wN = q; q += pe;
-    ctx->B.part = q;
-    if (cudaMalloc(&ctx->d_ctl, sizeof(Ctl)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
-    if (cudaMallocHost(&ctx->h_ctl, sizeof(Ctl)) != cudaSuccess) return bail(PEARL_ERR_CUDA);
-    std::memset(ctx->h_ctl, 0, sizeof(Ctl));
-    ctx->B.ctl = ctx->d_ctl;
-    if (ctx->use_tma && !build_tensor_maps(ctx)) ctx->use_tma = false;
-    ctx->stage_elems = 5 * (size_t)nx * ny;  // device staging is allocated at the first host transfer
-    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
-        return bail(PEARL_ERR_CUDA);
-    if (cudaMemcpy(ctx->d_ctl, ctx->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
-        return bail(PEARL_ERR_CUDA);
-    *out = ctx;
-    return PEARL_OK;
-}
-
-void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
-    if (!ctx) return;
-    cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    if (ctx->slab) cudaFree(ctx->slab);
-    if (ctx->d_ctl) cudaFree(ctx->d_ctl);
-    if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
-    if (ctx->d_stage) cudaFree(ctx->d_stage);
-    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-    delete ctx;
-}
-
-int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    ctx->stream = (cudaStream_t)stream;
-    return PEARL_OK;
-}
-
-int pearl_gpu_set_precision(pearl_gpu_ctx* ctx, int precision) {
-    if (!ctx || (precision != PEARL_PRECISION_FP64 && precision != PEARL_PRECISION_MIXED))
-        return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid precision");
-    ctx->P.mixed = precision == PEARL_PRECISION_MIXED;
-    return PEARL_OK;
-}
-
-int pearl_gpu_set_params(pearl_gpu_ctx* ctx, const pearl_params* params) {
-    if (!ctx || !params || !valid_params(params)) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid parameters");
-    ctx->params = *params;
-    fill_dev_params(ctx);
-    ctx->h_ctl->energy_valid = 0;
-    return push_ctl(ctx);
-}
-
-int pearl_gpu_upload(pearl_gpu_ctx* ctx, const double* phi, const double* carbon, const double* mu,
-                     const pearl_scalars* scalars) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    int rc = upload_set(ctx, ctx->h_ctl->cur, phi, carbon, mu);
-    if (rc) return rc;
-    if (scalars) ctx->h_ctl->S = *scalars;
-    ctx->h_ctl->energy_valid = 0;
-    rc = push_ctl(ctx);
-    if (rc) return rc;
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return PEARL_OK;
-}
-
-int pearl_gpu_download(pearl_gpu_ctx* ctx, double* phi, double* carbon, double* mu, pearl_scalars* scalars) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    int rc = download_set(ctx, ctx->h_ctl->cur, phi, carbon, mu);
-    if (rc) return rc;
-    if (scalars) *scalars = ctx->h_ctl->S;
-    return PEARL_OK;
-}
-
-int pearl_gpu_get_scalars(pearl_gpu_ctx* ctx, pearl_scalars* scalars) {
-    if (!ctx || !scalars) return PEARL_ERR_INVALID_ARGUMENT;
-    *scalars = ctx->h_ctl->S;
-    return PEARL_OK;
-}
-
-int pearl_gpu_set_scalars(pearl_gpu_ctx* ctx, const pearl_scalars* scalars) {
-    if (!ctx || !scalars) return PEARL_ERR_INVALID_ARGUMENT;
-    ctx->h_ctl->S = *scalars;
-    int rc = push_ctl(ctx);
-    if (rc) return rc;
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return PEARL_OK;
-}
-
-int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_report* report) {
-    if (!ctx || !limits || limits->max_steps < 1) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid run limits");
-    KArgs a{};
-    a.mode = kModeRun;
-    a.L = *limits;
-    int rc = launch(ctx, a);
-    if (report) {
-        report->steps = ctx->h_ctl->steps;
-        report->cg_total = ctx->h_ctl->cg_total;
-        report->cg_peak = ctx->h_ctl->cg_peak;
-        report->reached_stop = ctx->h_ctl->reached_stop;
-        report->last = ctx->h_ctl->last;
-    }
-    return rc;
-}
-
-int pearl_gpu_advance(pearl_gpu_ctx* ctx, double stop_time, pearl_step_info* out) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    pearl_run_limits L;
-    L.max_steps = 1;
-    L.config_max_steps = 0x7fffffffffffffffLL;
-    L.stop_time = stop_time;
-    L.end_time = INFINITY;
-    L.output_eps = 0;
-    pearl_run_report rep;
-    int rc = pearl_gpu_run(ctx, &L, &rep);
-    if (rc == PEARL_OK && rep.steps != 1) return fail(ctx, PEARL_ERR_INVALID_ADVANCE_TIME, "invalid advance time");
-    if (out) *out = rep.last;
-    return rc;
-}
-
-int pearl_gpu_maybe_shift(pearl_gpu_ctx* ctx, double trigger, double target, double c_gamma, int* rows) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeMaybeShift;
-    a.shift_trigger = trigger;
-    a.shift_target = target;
-    a.shift_c_gamma = c_gamma;
-    int rc = launch(ctx, a);
-    if (rows) *rows = rc == PEARL_OK ? ctx->h_ctl->iout[0] : 0;
-    return rc;
-}
-
-int pearl_gpu_snapshot(pearl_gpu_ctx* ctx, pearl_diag* out) {
-    if (!ctx || !out) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeSnapshot;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
-    const Ctl* h = ctx->h_ctl;
-    out->c_min = h->out[0];
-    out->c_max = h->out[1];
-    out->mu_min = h->out[2];
-    out->mu_max = h->out[3];
-    out->phi_sum_error = h->out[4];
-    out->mass = h->out[5];
-    out->energy = h->out[6];
-    out->ledger = out->mass + h->S.carbon_removed - h->S.carbon_added - h->S.initial_carbon;
-    return PEARL_OK;
-}
-
-int pearl_gpu_smooth_interface(pearl_gpu_ctx* ctx, int max_steps, int min_steps, double energy_rtol,
-                               double max_phase_change, pearl_smooth_report* out) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    // smooth_interface_only's control check (pearl_serial.cpp:874-876)
-    if (max_steps < 1 || min_steps < 0 || min_steps > max_steps || !(energy_rtol > 0) || !(max_phase_change > 0) ||
-        max_phase_change > .2)
-        return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid sharp-smoothing controls");
-    KArgs a{};
-    a.mode = kModeSmooth;
-    a.smooth_max_steps = max_steps;
-    a.smooth_min_steps = min_steps;
-    a.smooth_energy_rtol = energy_rtol;
-    a.smooth_max_phase_change = max_phase_change;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (out) {
-        const double* r = ctx->h_ctl->out;
-        out->steps = (int)r[0];
-        out->converged = (int)r[1];
-        out->energy_initial = r[2];
-        out->energy_final = r[3];
-        out->final_relative_energy_change = r[4];
-        out->final_max_phase_change = r[5];
-        for (int k = 0; k < 3; ++k) {
-            out->phase_fraction_before[k] = r[6 + k];
-            out->phase_fraction_after[k] = r[9 + k];
-        }
-    }
-    return PEARL_OK;
-}
-
-int pearl_gpu_mixture_sums(pearl_gpu_ctx* ctx, double* sum_c_intercept, double* sum_chi) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeMixSums;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
-    if (sum_c_intercept) *sum_c_intercept = ctx->h_ctl->out[0];
-    if (sum_chi) *sum_chi = ctx->h_ctl->out[1];
-    return PEARL_OK;
-}
-
-int pearl_gpu_init_composition(pearl_gpu_ctx* ctx, double mu, double* total_carbon) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeInitComposition;
-    a.init_mu = mu;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
-    if (total_carbon) *total_carbon = ctx->h_ctl->out[0];
-    return PEARL_OK;
-}
-
-int pearl_gpu_propose_phi(pearl_gpu_ctx* ctx, double dt, double* max_change) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModePropose;
-    a.dt = dt;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ctx->h_ctl->iout[1]) return fail(ctx, PEARL_ERR_SIMPLEX, "Simplex projection failed");
-    if (max_change) *max_change = ctx->h_ctl->out[0];
-    return PEARL_OK;
-}
-
-int pearl_gpu_upload_trial_phi(pearl_gpu_ctx* ctx, const double* phi) {
-    if (!ctx || !phi) return PEARL_ERR_INVALID_ARGUMENT;
-    int rc = upload_set(ctx, ctx->h_ctl->cur ^ 1, phi, nullptr, nullptr);
-    if (rc) return rc;
-    KArgs a{};
-    a.mode = kModeMix;
-    rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
-    return PEARL_OK;
-}
-
-int pearl_gpu_implicit_diffusion(pearl_gpu_ctx* ctx, double dt, int* ok, int* iterations, double* residual,
-                                 double* closure) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeDiffusion;
-    a.dt = dt;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ok) *ok = ctx->h_ctl->iout[0];
-    if (iterations) *iterations = ctx->h_ctl->iout[1];
-    if (residual) *residual = ctx->h_ctl->out[0];
-    if (closure) *closure = ctx->h_ctl->out[1];
-    return PEARL_OK;
-}
-
-int pearl_gpu_download_trial(pearl_gpu_ctx* ctx, double* phi, double* carbon, double* mu) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    return download_set(ctx, ctx->h_ctl->cur ^ 1, phi, carbon, mu);
-}
-
-int pearl_gpu_energy_mass(pearl_gpu_ctx* ctx, double* energy, double* mass) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeEnergy;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    if (ctx->h_ctl->iout[0]) return fail(ctx, PEARL_ERR_MIXTURE, "Invalid mixture coefficients");
-    if (energy) *energy = ctx->h_ctl->out[0];
-    if (mass) *mass = ctx->h_ctl->out[1];
-    return PEARL_OK;
-}
-
-int pearl_gpu_valid_state(pearl_gpu_ctx* ctx, int* valid) {
-    if (!ctx || !valid) return PEARL_ERR_INVALID_ARGUMENT;
-    KArgs a{};
-    a.mode = kModeValid;
-    int rc = launch(ctx, a);
-    if (rc) return rc;
-    *valid = ctx->h_ctl->iout[1] ? 0 : 1;
-    return PEARL_OK;
-}
-
-int pearl_gpu_selftest_division(int device, const double* a, const double* b, long long n,
-                                unsigned long long* mismatches) {
-    if (!a || !b || n < 0 || !mismatches) return PEARL_ERR_INVALID_ARGUMENT;
-    if (cudaSetDevice(device) != cudaSuccess) return PEARL_ERR_NO_DEVICE;
-    std::vector<double> rb((size_t)n);
-    for (long long i = 0; i < n; ++i) rb[(size_t)i] = 1.0 / b[i];
-    double *da = nullptr, *db = nullptr, *drb = nullptr;
-    unsigned long long* dm = nullptr;
-    const size_t bytes = (size_t)n * sizeof(double);
-    int rc = PEARL_OK;
-    if (cudaMalloc(&da, bytes) != cudaSuccess || cudaMalloc(&db, bytes) != cudaSuccess ||
-        cudaMalloc(&drb, bytes) != cudaSuccess || cudaMalloc(&dm, sizeof(unsigned long long)) != cudaSuccess)
-        rc = PEARL_ERR_CUDA;
-    if (rc == PEARL_OK && (cudaMemcpy(da, a, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
-                           cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
-                           cudaMemcpy(drb, rb.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
-                           cudaMemset(dm, 0, sizeof(unsigned long long)) != cudaSuccess))
-        rc = PEARL_ERR_CUDA;
-    if (rc == PEARL_OK) {
-        division_selftest_kernel<<<1184, 256>>>(da, db, drb, n, dm, 1);
-        if (cudaDeviceSynchronize() != cudaSuccess ||
-            cudaMemcpy(mismatches, dm, sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
-            rc = PEARL_ERR_CUDA;
-    }
-    cudaFree(da);
-    cudaFree(db);
-    cudaFree(drb);
-    cudaFree(dm);
-    return rc;
-}
-
-int pearl_gpu_selftest_wait_limit(pearl_gpu_ctx* ctx, int* status, double* waited_ms) {
-    if (!ctx || !status) return PEARL_ERR_INVALID_ARGUMENT;
-    PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    ctx->h_ctl->status = 0;
-    ctx->h_ctl->why = 0;
-    ctx->h_ctl->bar_count = 0;
-    int rc = push_ctl(ctx);
-    if (rc) return rc;
-    Ctl* ctl = ctx->d_ctl;
-    void* kargs[] = {&ctl};
-    PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)wait_limit_selftest_kernel, dim3(ctx->grid),
-                                             dim3(kThreads), kargs, 0, ctx->stream));
-    ctx->launches++;
-    PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-    rc = pull_ctl(ctx);
-    if (rc) return rc;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    if (waited_ms) *waited_ms = ms;
-    *status = ctx->h_ctl->status;
-    // leave the barrier words and status as a fresh context has them
-    ctx->h_ctl->status = 0;
-    ctx->h_ctl->why = 0;
-    ctx->h_ctl->bar_count = 0;
-    rc = push_ctl(ctx);
-    if (rc) return rc;
-    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return PEARL_OK;
-}
-
-int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* counts) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    for (int k = 0; k < 16; ++k) {
-        if (ms) ms[k] = k < kTagCount ? ctx->h_ctl->phase_ns[k] * 1e-6 : 0.0;
-        if (counts) counts[k] = k < kTagCount ? (long long)ctx->h_ctl->phase_count[k] : 0;
-    }
-    return PEARL_OK;
-}
-
-int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* launches, int* grid_blocks, double* last_ms) {
-    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
-    if (launches) *launches = ctx->launches;
-    if (grid_blocks) *grid_blocks = ctx->grid;
-    if (last_ms) *last_ms = ctx->last_ms;
-    return PEARL_OK;
-}
-
-}  // extern "C"
-
-// ============================================================ adjoint
-namespace {
-
-int launch_adjoint(pearl_gpu_ctx* ctx, AdjArgs& args) {
-    if (!ctx->adj_grid) {
-        int per_sm = 0, sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_adjoint_kernel, kThreads, 0));
-        if (per_sm < 1) return fail(ctx, PEARL_ERR_CUDA, "adjoint kernel cannot be resident");
-        const long long cells = (long long)ctx->nx * ctx->ny;
-        const long long want = (cells + kThreads - 1) / kThreads;
-        // the reduction partials of the context are sized for ctx->grid blocks
-        ctx->adj_grid = (int)std::max(1LL, std::min<long long>({want, (long long)per_sm * sms, (long long)ctx->grid}));
-    }
-    ctx->h_ctl->status = 0;
-    ctx->h_ctl->why = 0;
-    ctx->h_ctl->bar_count = 0;
-    int rc = push_ctl(ctx);
-    if (rc) return rc;
-    args.P = ctx->P;
-    args.B = ctx->B;
-    void* kargs[] = {&args};
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_adjoint_kernel, dim3(ctx->adj_grid), dim3(kThreads),
-                                             kargs, 0, ctx->stream));
-    ctx->launches++;
-    rc = pull_ctl(ctx);
-    if (rc) return rc;
-    if (ctx->h_ctl->status == PEARL_ERR_DEVICE_WAIT) {
-        ctx->h_ctl->bar_count = 0;
-        push_ctl(ctx);
-        return fail(ctx, PEARL_ERR_DEVICE_WAIT, "device grid barrier wait exceeded its limit");
-    }
-    return PEARL_OK;
-}
-
-}  // namespace
-
-extern "C" int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, int checkpoint_every,
-                                          const double* target_alpha, pearl_adjoint_report* out) {
-    if (!ctx || nsteps < 1 || checkpoint_every < 1 || !target_alpha || !out) return PEARL_ERR_INVALID_ARGUMENT;
-    if (ctx->params.phase_only) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "adjoint needs implicit diffusion");
-    if (ctx->P.mixed) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "adjoint differentiates the FP64 step");
-    PG_CUDA(ctx, cudaSetDevice(ctx->device));
-    std::memset(out, 0, sizeof *out);
-    const size_t pe = plane_elems(ctx);
-    const long long K = checkpoint_every;
-    const long long nseg = (nsteps + K - 1) / K;
-    const long long seglen = std::min(K, nsteps);
-    const size_t n_ckpt = (size_t)(nseg + 1) * 5 * pe, n_tape = (size_t)seglen * 6 * pe, n_adj = 23 * pe;
-    double* slab = nullptr;
-    PG_CUDA(ctx, cudaMalloc(&slab, (n_ckpt + n_tape + n_adj + (size_t)nsteps + 8) * sizeof(double)));
-    double* ckpt = slab;
-    double* tape = ckpt + n_ckpt;
-    double* adj = tape + n_tape;
-    double* dts = adj + n_adj;
-    double* acc = dts + nsteps;
-    AdjBufs J{};
-    {
-        double* q = adj;
-        for (int a = 0; a < 3; ++a, q += pe) J.bphi[a] = q;
-        J.bc = q; q += pe;
-        J.bmu = q; q += pe;
-        J.chi = q; q += pe;
-        J.K = q; q += pe;
-        J.ub = q; q += pe;
-        J.lam = q; q += pe;
-        J.r = q; q += pe;
-        J.z = q; q += pe;
-        J.p[0] = q; q += pe;
-        J.p[1] = q; q += pe;
-        J.Ap = q; q += pe;
-        J.diag = q; q += pe;
-        for (int a = 0; a < 3; ++a, q += pe) J.Fb[a] = q;
-        for (int a = 0; a < 3; ++a, q += pe) J.Ql[a] = q;
-    }
-    double* target = adj + 22 * pe;
-    std::vector<pearl_scalars> seg_scalars(nseg);
-    cudaEvent_t e[4];
-    for (auto& ev : e) cudaEventCreate(&ev);
-    auto state = [&](int set) { return ctx->B.phi[set][0]; };  // 5 contiguous planes
-    const Ctl initial_ctl = *ctx->h_ctl;
-    bool have_initial = false;
-    auto body = [&]() -> int {
-        PG_CUDA(ctx, cudaMemsetAsync(slab, 0, (n_ckpt + n_tape + n_adj + (size_t)nsteps + 8) * sizeof(double),
-                                     ctx->stream));
-        PG_CUDA(ctx, cudaMemcpy2DAsync(target, ctx->pitch * sizeof(double), target_alpha, ctx->nx * sizeof(double),
-                                       ctx->nx * sizeof(double), ctx->ny, cudaMemcpyHostToDevice, ctx->stream));
-        // forward with a checkpoint at the start of every segment
-        PG_CUDA(ctx, cudaEventRecord(e[0], ctx->stream));
-        for (long long seg = 0; seg < nseg; ++seg) {
-            const long long k0 = seg * K, len = std::min(K, nsteps - k0);
-            PG_CUDA(ctx, cudaMemcpyAsync(ckpt + (size_t)seg * 5 * pe, state(ctx->h_ctl->cur), 5 * pe * sizeof(double),
-                                         cudaMemcpyDeviceToDevice, ctx->stream));
-            have_initial = true;
-            seg_scalars[seg] = ctx->h_ctl->S;
-            KArgs a{};
-            a.mode = kModeRun;
-            a.L = pearl_run_limits{len, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
-            a.dt_log = dts + k0;
-            if (seg == nseg - 1) {
-                // the reverse sweep starts here: tape this segment now instead of recomputing it
-                a.tape = tape;
-                a.tape_slot = 6 * pe;
-            }
-            int rc = launch(ctx, a);
-            if (rc) return rc;
-            if (ctx->h_ctl->steps != len) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "forward stopped early");
-            out->cg_forward += ctx->h_ctl->cg_total;
-        }
-        PG_CUDA(ctx, cudaEventRecord(e[1], ctx->stream));
-        const Ctl final_ctl = *ctx->h_ctl;
-        PG_CUDA(ctx, cudaMemcpyAsync(ckpt + (size_t)nseg * 5 * pe, state(final_ctl.cur), 5 * pe * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
-        AdjArgs g{};
-        g.J = J;
-        g.target = target;
-        g.acc = acc;
-        g.obs_per_sigma = 16.0 / (std::acos(-1.0) * std::acos(-1.0) * ctx->params.epsilon);
-        g.two_eps = 2.0 * ctx->params.epsilon;
-        g.mode = 0;
-        g.ckpt = state(final_ctl.cur);
-        int rc = launch_adjoint(ctx, g);
-        if (rc) return rc;
-        // reverse sweep: recompute each segment from its checkpoint, then run it backwards
-        double recompute_ms = 0;
-        for (long long seg = nseg - 1; seg >= 0; --seg) {
-            const long long k0 = seg * K, len = std::min(K, nsteps - k0);
-            if (seg < nseg - 1) {
-                PG_CUDA(ctx, cudaMemcpyAsync(state(0), ckpt + (size_t)seg * 5 * pe, 5 * pe * sizeof(double),
-                                             cudaMemcpyDeviceToDevice, ctx->stream));
-                ctx->h_ctl->cur = 0;
-                ctx->h_ctl->S = seg_scalars[seg];
-                ctx->h_ctl->energy_valid = 0;
-                KArgs a{};
-                a.mode = kModeRun;
-                a.L = pearl_run_limits{len, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
-                a.forced_dt = dts + k0;
-                a.tape = tape;
-                a.tape_slot = 6 * pe;
-                rc = launch(ctx, a);
-                if (rc) return rc;
-                recompute_ms += ctx->last_ms;
-                if (ctx->h_ctl->steps != len)
-                    return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "recomputation stopped early");
-            }
-            g.mode = 1;
-            g.ckpt = ckpt + (size_t)seg * 5 * pe;
-            g.tape = tape;
-            g.slot = 6 * pe;
-            g.dts = dts + k0;
-            g.len = (int)len;
-            rc = launch_adjoint(ctx, g);
-            if (rc) return rc;
-        }
-        PG_CUDA(ctx, cudaEventRecord(e[2], ctx->stream));
-        // leave the forward's final state in the context
-        PG_CUDA(ctx, cudaMemcpyAsync(state(0), ckpt + (size_t)nseg * 5 * pe, 5 * pe * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, ctx->stream));
-        *ctx->h_ctl = final_ctl;
-        ctx->h_ctl->cur = 0;
-        ctx->h_ctl->energy_valid = 0;
-        rc = push_ctl(ctx);
-        if (rc) return rc;
-        double h_acc[8];
-        PG_CUDA(ctx, cudaMemcpyAsync(h_acc, acc, sizeof h_acc, cudaMemcpyDeviceToHost, ctx->stream));
-        PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        float f_ms = 0, b_ms = 0;
-        cudaEventElapsedTime(&f_ms, e[0], e[1]);
-        cudaEventElapsedTime(&b_ms, e[1], e[2]);
-        out->objective = h_acc[0];
-        out->grad[0] = h_acc[1];
-        out->grad[1] = h_acc[2];
-        out->grad[2] = h_acc[3];
-        out->cg_adjoint = (long long)h_acc[4];
-        out->steps = nsteps;
-        out->checkpoints = (int)nseg;
-        out->forward_ms = f_ms;
-        out->recompute_ms = recompute_ms;
-        out->adjoint_ms = b_ms - recompute_ms;
-        return PEARL_OK;
-    };
-    const int rc = body();
-    if (rc && have_initial) {
-        // a failed gradient leaves the context in its initial state
-        cudaMemcpyAsync(state(0), ckpt, 5 * pe * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
-        *ctx->h_ctl = initial_ctl;
-        ctx->h_ctl->cur = 0;
-        ctx->h_ctl->energy_valid = 0;
-        ctx->h_ctl->bar_count = 0;
-        push_ctl(ctx);
-    }
-    cudaStreamSynchronize(ctx->stream);
-    for (auto& ev : e) cudaEventDestroy(ev);
-    cudaFree(slab);
-    return rc;
-}
-
-// ============================================================ batched instances
-struct pearl_gpu_batch {
-    int device = 0, n = 0;
-    std::vector<pearl_gpu_ctx*> inst;  // host bookkeeping and buffers of every instance
-    Ctl* d_ctls = nullptr;             // the instances' control blocks, contiguous
-    Ctl* h_ctls = nullptr;             // pinned mirror
-    BatchInstance* d_inst = nullptr;
-    int* d_order = nullptr;
-    int* d_first = nullptr;
-    Ctl* d_group_ctl = nullptr;
-    double* d_group_part = nullptr;
-    int per_sm = 0, sms = 0, grid = 0, group_blocks = 0, ngroups = 0;
-    bool use_tma = true;      // TMA staging in use (needs the 32x16 tile)
-    bool tma_capable = true;  // tensor maps of every instance encoded and the shared memory granted
-    int tile_wx = 0;          // tile shape of every instance: 2^tile_wx warps side by side in x
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double last_ms = 0;
-    long long launches = 0;
-    std::string error;
-};
-
-namespace {
-
-int bfail(pearl_gpu_batch* b, int status, const std::string& msg) {
-    if (b) b->error = msg;
-    return status;
-}
-#define PB_CUDA(b, call)                                                                        \
-    do {                                                                                        \
-        cudaError_t e_ = (call);                                                                \
-        if (e_ != cudaSuccess) return bfail(b, PEARL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-// Give every instance the tile shape `wx`, split the cooperative grid into
-// groups of `gb` blocks and hand out the instances longest-first to the
-// least-loaded group (cost ~ cells).  TMA staging needs the 32x16 tile.
-int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma, int wx) {
-    const int max_grid = b->per_sm * b->sms;
-    if (gb < 1 || gb > max_grid) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid group size");
-    if (wx < 0 || wx > 3) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid tile shape");
-    b->group_blocks = gb;
-    b->ngroups = max_grid / gb;
-    b->grid = b->ngroups * gb;
-    b->tile_wx = wx;
-    b->use_tma = use_tma && wx == 0 && b->tma_capable;
-    for (auto* c : b->inst) set_tile_shape(c, wx);
-    std::vector<int> idx(b->n);
-    for (int i = 0; i < b->n; ++i) idx[i] = i;
-    std::sort(idx.begin(), idx.end(), [&](int x, int y) {
-        return (long long)b->inst[x]->nx * b->inst[x]->ny > (long long)b->inst[y]->nx * b->inst[y]->ny;
-    });
-    std::vector<double> load(b->ngroups, 0.0);
-    std::vector<std::vector<int>> lists(b->ngroups);
-    for (int i : idx) {
-        // a group's blocks share an instance's tiles: cost = cells / min(blocks, tiles)
-        const pearl_gpu_ctx* c = b->inst[i];
-        const double cells = (double)c->nx * c->ny;
-        const double cost = cells / std::max(1, std::min(gb, c->P.ntiles));
-        int best = 0;
-        for (int g = 1; g < b->ngroups; ++g)
-            if (load[g] < load[best]) best = g;
-        load[best] += cost;
-        lists[best].push_back(i);
-    }
-    std::vector<int> order, first(1, 0);
-    for (int g = 0; g < b->ngroups; ++g) {
-        order.insert(order.end(), lists[g].begin(), lists[g].end());
-        first.push_back((int)order.size());
-    }
-    cudaFree(b->d_order);
-    cudaFree(b->d_first);
-    cudaFree(b->d_group_ctl);
-    cudaFree(b->d_group_part);
-    b->d_order = nullptr;
-    b->d_first = nullptr;
-    b->d_group_ctl = nullptr;
-    b->d_group_part = nullptr;
-    PB_CUDA(b, cudaMalloc(&b->d_order, sizeof(int) * std::max(1, b->n)));
-    PB_CUDA(b, cudaMalloc(&b->d_first, sizeof(int) * first.size()));
-    PB_CUDA(b, cudaMalloc(&b->d_group_ctl, sizeof(Ctl) * b->ngroups));
-    PB_CUDA(b, cudaMalloc(&b->d_group_part, sizeof(double) * (size_t)b->ngroups * 2 * gb * kMaxRed));
-    PB_CUDA(b, cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
-    PB_CUDA(b, cudaMemcpy(b->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
-    PB_CUDA(b, cudaMemset(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups));
-    // per-instance descriptors (tensor maps, parameters, buffers)
-    std::vector<BatchInstance> hi(b->n);
-    for (int i = 0; i < b->n; ++i) {
-        std::memcpy(hi[i].maps, b->inst[i]->maps, sizeof hi[i].maps);
-        hi[i].P = b->inst[i]->P;
-        hi[i].B = b->inst[i]->B;
-    }
-    PB_CUDA(b, cudaMemcpy(b->d_inst, hi.data(), sizeof(BatchInstance) * b->n, cudaMemcpyHostToDevice));
-    return PEARL_OK;
-}
-
-int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
-    PB_CUDA(b, cudaSetDevice(b->device));
-    PB_CUDA(b, cudaMemsetAsync(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups, b->stream));
-    BatchArgs args{};
-    args.inst = b->d_inst;
-    args.order = b->d_order;
-    args.first = b->d_first;
-    args.group_blocks = b->group_blocks;
-    args.group_ctl = b->d_group_ctl;
-    args.group_part = b->d_group_part;
-    args.use_tma = b->use_tma ? 1 : 0;
-    args.L = L;
-    void* kargs[] = {&args};
-    PB_CUDA(b, cudaEventRecord(b->ev0, b->stream));
-    PB_CUDA(b, cudaLaunchCooperativeKernel((const void*)pearl_batch_kernel, dim3(b->grid), dim3(kThreads), kargs,
-                                           b->use_tma ? kTmaSmemBytes : 0, b->stream));
-    b->launches++;
-    PB_CUDA(b, cudaEventRecord(b->ev1, b->stream));
-    PB_CUDA(b, cudaMemcpyAsync(b->h_ctls, b->d_ctls, sizeof(Ctl) * b->n, cudaMemcpyDeviceToHost, b->stream));
-    PB_CUDA(b, cudaStreamSynchronize(b->stream));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
-    b->last_ms = ms;
-    for (int i = 0; i < b->n; ++i) *b->inst[i]->h_ctl = b->h_ctls[i];
-    return PEARL_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-void pearl_gpu_batch_destroy(pearl_gpu_batch* b) {
-    if (!b) return;
-    cudaSetDevice(b->device);
-    if (b->stream) cudaStreamSynchronize(b->stream);
-    for (auto* c : b->inst) {
-        if (c) c->d_ctl = nullptr;  // owned by the batch
-        pearl_gpu_destroy(c);
-    }
-    cudaFree(b->d_ctls);
-    if (b->h_ctls) cudaFreeHost(b->h_ctls);
-    cudaFree(b->d_inst);
-    cudaFree(b->d_order);
-    cudaFree(b->d_first);
-    cudaFree(b->d_group_ctl);
-    cudaFree(b->d_group_part);
-    if (b->ev0) cudaEventDestroy(b->ev0);
-    if (b->ev1) cudaEventDestroy(b->ev1);
-    delete b;
-}
-
-int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, const int* ny, int device,
-                           int group_blocks, pearl_gpu_batch** out) {
-    if (!out || n < 1 || !params || !nx || !ny) return PEARL_ERR_INVALID_ARGUMENT;
-    *out = nullptr;
-    pearl_gpu_batch* b = new pearl_gpu_batch();
-    b->device = device;
-    b->n = n;
-    auto bail = [&](int rc) {
-        pearl_gpu_batch_destroy(b);
-        return rc;
-    };
-    if (cudaSetDevice(device) != cudaSuccess) return bail(PEARL_ERR_NO_DEVICE);
-    b->inst.assign(n, nullptr);
-    if (cudaMalloc(&b->d_ctls, sizeof(Ctl) * n) != cudaSuccess ||
-        cudaMallocHost(&b->h_ctls, sizeof(Ctl) * n) != cudaSuccess ||
-        cudaMalloc(&b->d_inst, sizeof(BatchInstance) * n) != cudaSuccess)
-        return bail(PEARL_ERR_CUDA);
-    std::memset(b->h_ctls, 0, sizeof(Ctl) * n);
-    bool tma = true;
-    for (int i = 0; i < n; ++i) {
-        const int rc = pearl_gpu_create(&params[i], nx[i], ny[i], device, &b->inst[i]);
-        if (rc) return bail(rc);
-        pearl_gpu_ctx* c = b->inst[i];
-        cudaFree(c->d_ctl);  // the batch keeps every control block in one array
-        c->d_ctl = b->d_ctls + i;
-        c->B.ctl = c->d_ctl;
-        if (cudaMemcpy(c->d_ctl, c->h_ctl, sizeof(Ctl), cudaMemcpyHostToDevice) != cudaSuccess)
-            return bail(PEARL_ERR_CUDA);
-        tma = tma && c->use_tma;
-    }
-    if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
-        return bail(PEARL_ERR_CUDA);
-    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
-    if (tma &&
-        cudaFuncSetAttribute(pearl_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
-            cudaSuccess)
-        tma = false;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->per_sm, pearl_batch_kernel, kThreads,
-                                                      tma ? kTmaSmemBytes : 0) != cudaSuccess ||
-        b->per_sm < 1)
-        return bail(PEARL_ERR_CUDA);
-    b->tma_capable = tma;
-    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : 4, tma, 0);
-    if (rc) return bail(rc);
-    *out = b;
-    return PEARL_OK;
-}
-
-int pearl_gpu_batch_upload(pearl_gpu_batch* b, int i, const double* phi, const double* carbon, const double* mu,
-                           const pearl_scalars* scalars) {
-    if (!b || i < 0 || i >= b->n) return PEARL_ERR_INVALID_ARGUMENT;
-    const int rc = pearl_gpu_upload(b->inst[i], phi, carbon, mu, scalars);
-    if (rc) return bfail(b, rc, pearl_gpu_last_error(b->inst[i]));
-    return PEARL_OK;
-}
-
-int pearl_gpu_batch_download(pearl_gpu_batch* b, int i, double* phi, double* carbon, double* mu,
-                             pearl_scalars* scalars) {
-    if (!b || i < 0 || i >= b->n) return PEARL_ERR_INVALID_ARGUMENT;
-    const int rc = pearl_gpu_download(b->inst[i], phi, carbon, mu, scalars);
-    if (rc) return bfail(b, rc, pearl_gpu_last_error(b->inst[i]));
-    return PEARL_OK;
-}
-
-int pearl_gpu_batch_run(pearl_gpu_batch* b, const pearl_run_limits* limits, pearl_run_report* reports,
-                        int* status) {
-    if (!b || !limits || limits->max_steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
-    int rc = batch_launch(b, *limits);
-    if (rc) return rc;
-    int first_bad = PEARL_OK;
-    for (int i = 0; i < b->n; ++i) {
-        const Ctl& h = b->h_ctls[i];
-        if (reports) {
-            reports[i].steps = h.steps;
-            reports[i].cg_total = h.cg_total;
-            reports[i].cg_peak = h.cg_peak;
-            reports[i].reached_stop = h.reached_stop;
-            reports[i].last = h.last;
-        }
-        if (status) status[i] = h.status;
-        if (h.status == PEARL_ERR_DEVICE_WAIT) first_bad = PEARL_ERR_DEVICE_WAIT;
-    }
-    if (first_bad) return bfail(b, first_bad, "device grid barrier wait exceeded its limit");
-    return PEARL_OK;
-}
-
-int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, int* use_tma, int* tile_warps_x) {
-    if (!b || steps < 1) return PEARL_ERR_INVALID_ARGUMENT;
-    PB_CUDA(b, cudaSetDevice(b->device));
-    // back up every instance's current state (5 planes) and control block
-    std::vector<double*> backup(b->n, nullptr);
-    auto release = [&]() {
-        for (double* p : backup) cudaFree(p);
-    };
-    for (int i = 0; i < b->n; ++i) {
-        pearl_gpu_ctx* c = b->inst[i];
-        const size_t bytes = 5 * plane_elems(c) * sizeof(double);
-        if (cudaMalloc(&backup[i], bytes) != cudaSuccess) {
-            release();
-            return bfail(b, PEARL_ERR_CUDA, "autotune backup allocation");
-        }
-        cudaMemcpyAsync(backup[i], c->B.phi[c->h_ctl->cur][0], bytes, cudaMemcpyDeviceToDevice, b->stream);
-    }
-    // the instances' host control blocks are authoritative (uploads update them)
-    std::vector<Ctl> saved(b->n);
-    for (int i = 0; i < b->n; ++i) saved[i] = *b->inst[i]->h_ctl;
-    double best_ms = 1e300;
-    int best_gb = b->group_blocks, best_wx = b->tile_wx;
-    bool best_tma = b->use_tma;
-    const int cands[] = {1, 2, 4, 8, 16};
-    pearl_run_limits L{1, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
-    // tile shapes 32x16 (with and without TMA staging), 64x8 and 128x4
-    struct Shape {
-        int wx;
-        bool tma;
-    };
-    std::vector<Shape> shapes;
-    if (b->tma_capable) shapes.push_back({0, true});
-    shapes.push_back({0, false});
-    shapes.push_back({1, false});
-    shapes.push_back({2, false});
-    for (const Shape& sh : shapes) {
-        const int tma = sh.tma ? 1 : 0;
-        for (int gb : cands) {
-            if (gb > b->per_sm * b->sms) continue;
-            int rc = batch_configure(b, gb, tma != 0, sh.wx);
-            double ms = 0;
-            for (int s = 0; rc == PEARL_OK && s < steps; ++s) {
-                rc = batch_launch(b, L);
-                ms += b->last_ms;
-            }
-            // restore
-            for (int i = 0; i < b->n; ++i) {
-                pearl_gpu_ctx* c = b->inst[i];
-                cudaMemcpyAsync(c->B.phi[saved[i].cur][0], backup[i], 5 * plane_elems(c) * sizeof(double),
-                                cudaMemcpyDeviceToDevice, b->stream);
-            }
-            std::memcpy(b->h_ctls, saved.data(), sizeof(Ctl) * b->n);
-            cudaMemcpyAsync(b->d_ctls, b->h_ctls, sizeof(Ctl) * b->n, cudaMemcpyHostToDevice, b->stream);
-            cudaStreamSynchronize(b->stream);
-            for (int i = 0; i < b->n; ++i) *b->inst[i]->h_ctl = saved[i];
-            if (rc) {
-                release();
-                return rc;
-            }
-            if (ms < best_ms) {
-                best_ms = ms;
-                best_gb = gb;
-                best_tma = tma != 0;
-                best_wx = sh.wx;
-            }
-        }
-    }
-    release();
-    const int rc = batch_configure(b, best_gb, best_tma, best_wx);
-    if (group_blocks) *group_blocks = best_gb;
-    if (use_tma) *use_tma = best_tma ? 1 : 0;
-    if (tile_warps_x) *tile_warps_x = 1 << best_wx;
-    return rc;
-}
-
-int pearl_gpu_batch_configure(pearl_gpu_batch* b, int group_blocks, int use_tma, int tile_warps_x) {
-    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
-    const int wx = tile_warps_x == 1 ? 0 : tile_warps_x == 2 ? 1 : tile_warps_x == 4 ? 2 : tile_warps_x == 8 ? 3 : -1;
-    if (wx < 0) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "tile_warps_x must be 1, 2, 4 or 8");
-    PB_CUDA(b, cudaSetDevice(b->device));
-    return batch_configure(b, group_blocks, use_tma != 0, wx);
-}
-
-int pearl_gpu_batch_set_precision(pearl_gpu_batch* b, int precision) {
-    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
-    for (auto* c : b->inst) {
-        const int rc = pearl_gpu_set_precision(c, precision);
-        if (rc) return bfail(b, rc, "invalid precision");
-    }
-    return batch_configure(b, b->group_blocks, b->use_tma, b->tile_wx);
-}
-
-int pearl_gpu_batch_stats(const pearl_gpu_batch* b, long long* launches, int* grid_blocks, int* group_blocks,
-                          double* last_kernel_ms) {
-    if (!b) return PEARL_ERR_INVALID_ARGUMENT;
-    if (launches) *launches = b->launches;
-    if (grid_blocks) *grid_blocks = b->grid;
-    if (group_blocks) *group_blocks = b->group_blocks;
-    if (last_kernel_ms) *last_kernel_ms = b->last_ms;
-    return PEARL_OK;
-}
-
-const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* b) { return b ? b->error.c_str() : "null batch"; }
-
-}  // extern "C"
-
-// ============================================================ no-allocation entry point
-// pearl_gpu_advance_noalloc runs the same persistent kernel as pearl_gpu_advance
-// for callers that must not allocate device memory themselves or through this
-// library: programs whose device memory belongs to another allocator (a
-// framework's caching pool, a fixed per-process budget) and latency-critical
-// loops that cannot afford cudaMalloc/cudaFree, which may synchronise the
-// device.  The caller passes the state planes in device memory; every scratch
-// buffer (the trial state, the implicit-solve vectors, the reduction partials
-// and the control block) is carved from one fixed array compiled into this
-// library, which each GPU that loads the library keeps until the process exits.
-namespace {
-
-constexpr long long kNoAllocMaxCells = 262144;  // 512 x 512 cells
-constexpr int kNoAllocMaxBlocks = 4096;         // bound of the cooperative grid
-constexpr int kNoAllocPlanes = 17;  // trial phi(3) c mu + K chi icpt diag x r z p0 p1 Ap wE wN
-constexpr size_t kNoAllocCtlDoubles = (sizeof(Ctl) + 255) / 256 * 32;
-constexpr size_t kNoAllocDoubles =
-    kNoAllocPlanes * (size_t)kNoAllocMaxCells + (size_t)2 * kNoAllocMaxBlocks * kMaxRed + kNoAllocCtlDoubles;
-constexpr int kNoAllocMaxDevices = 64;
-
-std::mutex g_noalloc_mutex;
-double* g_noalloc_device_ptr[kNoAllocMaxDevices] = {};
-
-}  // namespace
-
-// 17 planes of 262144 doubles + partials + control block: about 36 MB per GPU.
-static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
-
-namespace {
-
-// Device address of g_noalloc_scratch on the current device, looked up once per
-// device.  The host-side name is only a stand-in for the device symbol, so the
-// address must come from cudaGetSymbolAddress with that device current.
-int noalloc_scratch(int device, double** out) {
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (device < 0 || device >= kNoAllocMaxDevices) return PEARL_ERR_NO_DEVICE;
-    if (!g_noalloc_device_ptr[device]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PEARL_ERR_CUDA;
-        g_noalloc_device_ptr[device] = static_cast<double*>(p);
-    }
-    *out = g_noalloc_device_ptr[device];
-    return PEARL_OK;
-}
-
-}  // namespace
-
-extern "C" int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double* d_phi,
-                                         double* d_carbon, double* d_mu, pearl_scalars* scalars,
-                                         double stop_time, pearl_step_info* out, void* stream) {
-    if (!params || !d_phi || !d_carbon || !d_mu || !scalars || nx < 3 || ny < 2 || !valid_params(params))
-        return PEARL_ERR_INVALID_ARGUMENT;
-    if ((long long)nx * ny > kNoAllocMaxCells) return PEARL_ERR_TOO_LARGE;
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) return PEARL_ERR_NO_DEVICE;
-    double* scratch = nullptr;
-    int rc = noalloc_scratch(device, &scratch);
-    if (rc) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-
-    // Parameters and buffer table on the stack; nothing is allocated.
-    pearl_gpu_ctx ctx;
-    ctx.device = device;
-    ctx.nx = nx;
-    ctx.ny = ny;
-    ctx.pitch = nx;  // the caller's planes are dense rows of nx doubles
-    ctx.params = *params;
-    fill_dev_params(&ctx);
-    const size_t pe = (size_t)nx * ny;
-    DevBufs& B = ctx.B;
-    for (int a = 0; a < 3; ++a) B.phi[0][a] = d_phi + (size_t)a * pe;
-    B.c[0] = d_carbon;
-    B.mu[0] = d_mu;
-    double* q = scratch;
-    for (int a = 0; a < 3; ++a, q += pe) B.phi[1][a] = q;
-    B.c[1] = q; q += pe;
-    B.mu[1] = q; q += pe;
-    B.K = q; q += pe;
-    B.chi = q; q += pe;
-    B.icpt = q; q += pe;
-    B.diag = q; q += pe;
-    B.x = q; q += pe;
-    B.r = q; q += pe;
-    B.z = q; q += pe;
-    B.p[0] = q; q += pe;
-    B.p[1] = q; q += pe;
-    B.Ap = q; q += pe;
-    B.wE = q; q += pe;
-    B.wN = q;
-    B.part = scratch + kNoAllocPlanes * (size_t)kNoAllocMaxCells;
-    B.ctl = reinterpret_cast<Ctl*>(B.part + (size_t)2 * kNoAllocMaxBlocks * kMaxRed);
-
-    int sms = 0, per_sm = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads, 0) != cudaSuccess ||
-        per_sm < 1)
-        return PEARL_ERR_CUDA;
-    const int grid = std::max(1, std::min(std::min(per_sm * sms, ctx.P.ntiles), kNoAllocMaxBlocks));
-
-    // The scratch keeps the previous call's contents: reset the control block
-    // (status, barrier counter, cached energies) before the launch.
-    Ctl h;
-    std::memset(&h, 0, sizeof h);
-    h.S = *scalars;
-    h.cur = 0;
-    h.energy_valid = 0;
-    if (cudaMemcpyAsync(B.ctl, &h, sizeof h, cudaMemcpyHostToDevice, st) != cudaSuccess) return PEARL_ERR_CUDA;
-
-    KArgs a{};
-    a.P = ctx.P;
-    a.B = B;
-    a.mode = kModeRun;
-    a.L.max_steps = 1;
-    a.L.config_max_steps = 0x7fffffffffffffffLL;
-    a.L.stop_time = stop_time;
-    a.L.end_time = INFINITY;
-    a.L.output_eps = 0;
-    void* kargs[] = {&a};
-    if (cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(grid), dim3(kThreads), kargs, 0, st) !=
-        cudaSuccess)
-        return PEARL_ERR_CUDA;
-    if (cudaMemcpyAsync(&h, B.ctl, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return PEARL_ERR_CUDA;
-    if (h.status != PEARL_OK) return h.status;
-    if (h.steps != 1) return PEARL_ERR_INVALID_ADVANCE_TIME;
-    // The accepted state sits in the scratch set; copy it into the caller's planes.
-    if (h.cur == 1) {
-        if (cudaMemcpyAsync(d_phi, B.phi[1][0], 3 * pe * sizeof(double), cudaMemcpyDeviceToDevice, st) !=
-                cudaSuccess ||
-            cudaMemcpyAsync(d_carbon, B.c[1], pe * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-            cudaMemcpyAsync(d_mu, B.mu[1], pe * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
-            return PEARL_ERR_CUDA;
-    }
-    *scalars = h.S;
-    if (out) *out = h.last;
-    return PEARL_OK;
-}

@@ -1,0 +1,59 @@
+// pearl_host.hpp — host-side context of one device-resident domain and the
+// helpers the host files share (pearl_ctx.cu defines them).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "pearl_kernels.cuh"
+
+struct pearl_gpu_ctx {
+    CUtensorMap maps[pearl_gpu::kMapCount];
+    bool use_tma = false;
+    int device = 0;
+    int nx = 0, ny = 0, pitch = 0;
+    cudaStream_t stream = nullptr;
+    pearl_params params{};
+    pearl_gpu::DevParams P{};
+    pearl_gpu::DevBufs B{};
+    double* slab = nullptr;
+    pearl_gpu::Ctl* d_ctl = nullptr;
+    pearl_gpu::Ctl* h_ctl = nullptr;  // pinned
+    double* d_stage = nullptr;  // dense device staging of one host state (5 n doubles)
+    size_t stage_elems = 0;
+    int grid = 0;
+    long long launches = 0;
+    double last_ms = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int adj_grid = 0;  // cooperative grid of the adjoint kernel (0 until first use)
+    std::string error;
+};
+
+namespace pearl_gpu {
+
+constexpr int kDefaultWarpsXLog2 = 0;
+
+const char* why_text(int why);
+int fail(pearl_gpu_ctx* ctx, int status, const std::string& msg);
+int cuda_fail(pearl_gpu_ctx* ctx, cudaError_t e, const char* what);
+bool valid_params(const pearl_params* p);
+double host_psi(const pearl_params* p, int a, double mu);
+// Tile of (32 << wx) x (2 << (3 - wx)) cells: 2^wx warps side by side in x.
+void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2);
+void fill_dev_params(pearl_gpu_ctx* ctx);
+int pull_ctl(pearl_gpu_ctx* ctx);
+int push_ctl(pearl_gpu_ctx* ctx);
+// Launch the persistent kernel in args.mode; on return h_ctl holds the device
+// control block.  Maps the device status to the reference's messages.
+int launch(pearl_gpu_ctx* ctx, KArgs& args);
+size_t plane_elems(const pearl_gpu_ctx* ctx);
+bool build_tensor_maps(pearl_gpu_ctx* ctx);
+
+}  // namespace pearl_gpu
+
+#define PG_CUDA(ctx, call)                                  \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)

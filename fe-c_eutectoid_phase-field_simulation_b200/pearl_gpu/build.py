@@ -25,7 +25,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # FP64 path: -fmad=false keeps every multiply and add separately rounded, as in
 # the reference built for plain x86-64, so per-cell results match bitwise.
 CU_SOURCES = {
-    "pearl_fp64.cu": ["-fmad=false"],
+    "pearl_fp64.cu": ["-fmad=false"],        # phases and kernels
+    "pearl_ctx.cu": ["-fmad=false"],         # context, transfers, single-domain C ABI
+    "pearl_batch.cu": ["-fmad=false"],       # batched instances
+    "pearl_adjoint_host.cu": ["-fmad=false"],  # adjoint gradient driver
+    "pearl_noalloc.cu": ["-fmad=false"],     # step without device allocation
 }
 # host driver (the pearl_gpu executable): C++17, linked against libpearl_gpu.so
 CLI_SOURCES = ["config.cpp", "io.cpp", "main.cpp"]
@@ -43,7 +47,7 @@ def _newer(out: Path, inputs: list[Path]) -> bool:
 
 
 def sources() -> list[Path]:
-    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h"))
+    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.hpp"))
     deps += list(HOST.glob("*.cpp")) + list(HOST.glob("*.hpp")) + list(INCLUDE.glob("*.h"))
     return deps
 
