@@ -255,10 +255,17 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
     planes[kMapR] = B.r;
     planes[kMapAp] = B.Ap;
     planes[kMapDiag] = B.diag;
+    planes[kMapXc] = B.x;
+    planes[kMapP0c] = B.p[0];
+    planes[kMapP1c] = B.p[1];
+    planes[kMapRc] = B.r;
+    planes[kMapApc] = B.Ap;
+    planes[kMapDiagc] = B.diag;
     for (int m = 0; m < kMapCount; ++m) {
         const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
         const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(double)};
-        const cuuint32_t box[2] = {(cuuint32_t)kBoxW, (cuuint32_t)kBoxH};
+        const bool tile_only = m >= kMapXc;
+        const cuuint32_t box[2] = {(cuuint32_t)(tile_only ? kTileX : kBoxW), (cuuint32_t)(tile_only ? kTileRows : kBoxH)};
         const cuuint32_t estr[2] = {1, 1};
         if (encode(&ctx->maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, planes[m], dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

@@ -219,6 +219,8 @@ constexpr size_t kTmaSmemBytes = 128 + kPipeDoubles * sizeof(double);
 enum MapId : int {
     kMapState = 0,  // + 5*set + field
     kMapK = 10, kMapChi, kMapIcpt, kMapX, kMapZ, kMapP0, kMapP1, kMapWE, kMapWN, kMapR, kMapAp, kMapDiag,
+    // tile-only boxes (kTileX x kTileRows, no halo) for the pointwise CG update
+    kMapXc, kMapP0c, kMapP1c, kMapRc, kMapApc, kMapDiagc,
     kMapCount
 };
 

@@ -307,13 +307,14 @@ struct SmemSrc {
     const double* base;  // stage base: field k at base + k*kFieldStride
     int lx, ly0;         // box column of x, box row of the lower cell
     bool south, v1, north1;
+    int w;               // box row length (kBoxW with halo, kTileX without)
     __device__ __forceinline__ double v(int k, int cell, int dir) const {
         int ly = ly0 + cell, x = lx;
         if (dir == kW) x -= 1;
         if (dir == kE) x += 1;
         if (dir == kS) ly = cell == 0 ? (south ? ly - 1 : ly) : ly - 1;
         if (dir == kN) ly = cell == 0 ? (v1 ? ly + 1 : ly) : (north1 ? ly + 1 : ly);
-        return base[k * kFieldStride + ly * kBoxW + x];
+        return base[k * kFieldStride + ly * w + x];
     }
 };
 
@@ -372,7 +373,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // tensor map maps[k]; slots whose bit is set in `stencil` also get the
 // periodic x wrap patched from `planes`.  Returns false after a bounded wait
 // ran out (the status is recorded; in-flight copies are drained, bounded).
-template <int NF, class Body>
+template <int NF, bool kTileOnly = false, class Body>
 __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const double* const (&planes)[NF],
                       unsigned stencil, Body&& body) {
     const DevParams& P = a.P;
@@ -401,10 +402,12 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
         const int s = k % S;
         double* dst = pp.stage + (size_t)s * NF * kFieldStride;
         fence_proxy_async();  // earlier plain stores (global, and the stage's patch) before these async reads/writes
-        mbar_arrive_expect_tx(&pp.bar[s], NF * kBoxBytes);
+        // tile-only boxes start at the tile (x multiple of 32 doubles); halo boxes two cells left, one row up
+        mbar_arrive_expect_tx(&pp.bar[s], NF * (kTileOnly ? kTileX * kTileRows * (uint32_t)sizeof(double) : kBoxBytes));
 #pragma unroll
         for (int f = 0; f < NF; ++f)
-            tma_load_2d(dst + f * kFieldStride, &a.maps[maps[f]], bx * kTileX - 2, by * kTileRows - 1, &pp.bar[s]);
+            tma_load_2d(dst + f * kFieldStride, &a.maps[maps[f]], bx * kTileX - (kTileOnly ? 0 : 2),
+                        by * kTileRows - (kTileOnly ? 0 : 1), &pp.bar[s]);
     };
     for (int k = 0; k < S - 1 && k < nb; ++k) issue(k);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -436,7 +439,8 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
         }
         const Pair c = pair_of(P, t);
         if (c.v0) {
-            SmemSrc<NF> src{st, lane + 2, 2 * warp + 1, c.y0 > 0, c.v1, c.y0 + 2 < P.ny};
+            SmemSrc<NF> src = kTileOnly ? SmemSrc<NF>{st, lane, 2 * warp, c.y0 > 0, c.v1, c.y0 + 2 < P.ny, kTileX}
+                                        : SmemSrc<NF>{st, lane + 2, 2 * warp + 1, c.y0 > 0, c.v1, c.y0 + 2 < P.ny, kBoxW};
             body(src, c);
         }
         __syncthreads();
@@ -761,9 +765,9 @@ __device__ bool phase_apply(const Dom& a, Red& red, double dt, bool first, doubl
 __device__ bool phase_update(const Dom& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
     const DevBufs& B = a.B;
     double s0 = 0, s1 = 0;
-    const int maps[5] = {kMapX, pcur ? kMapP1 : kMapP0, kMapR, kMapAp, kMapDiag};
+    const int maps[5] = {kMapXc, pcur ? kMapP1c : kMapP0c, kMapRc, kMapApc, kMapDiagc};
     const double* const planes[5] = {B.x, B.p[pcur], B.r, B.Ap, B.diag};
-    const bool ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x0u, [&](const auto& src, const Pair& c) {
+    const bool ok = sweep<5, true>(a, *red.pipe_ptr, maps, planes, 0x0u, [&](const auto& src, const Pair& c) {
         {
             const double x = src.v(0, 0, kC) + alpha * src.v(1, 0, kC), r = src.v(2, 0, kC) - alpha * src.v(3, 0, kC);
             const double z = r / src.v(4, 0, kC);
