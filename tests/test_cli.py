@@ -177,3 +177,29 @@ def test_cli_smoke_run_matches_reference(cli, tmp_path):
     assert np.abs(fields["mu"] - ref_fields["mu"]).max() <= 1e-5
     c, c_ref = fields["carbon"], ref_fields["carbon"]
     assert abs(c.sum() - c_ref.sum()) <= 1e-12 * abs(c_ref.sum())
+
+
+@pytest.mark.gpu
+def test_cli_stop_restart_is_bitwise(cli, tmp_path):
+    """Restart equivalence (VALIDATION.md:33-35): 12 steps, then a restart from
+    that checkpoint for 12 more, equal an uninterrupted 24-step run bitwise."""
+    from golden.make_cli_golden import read_container
+
+    lines = cli_inputs.case_lamella_linear_gp()
+    inp = cli_inputs.write_input(tmp_path / "a.in", lines)
+
+    def run(out, *args):
+        p = subprocess.run([str(cli), str(inp), str(tmp_path / out), *args], capture_output=True, text=True)
+        assert p.returncode == 0, p.stderr
+        return tmp_path / out
+
+    whole = run("whole", "--max-steps", "24")
+    first = run("first", "--max-steps", "12")
+    second = run("second", "--restart", str(first / "checkpoint.h5"), "--max-steps", "12")
+    a, b = read_container(whole / "checkpoint.h5"), read_container(second / "checkpoint.h5")
+    assert sorted(a) == sorted(b)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    wa, wb = (whole / "STOPPED.txt").read_text().splitlines(), (second / "STOPPED.txt").read_text().splitlines()
+    for k in (1, 2, 4):  # time, step, rejected (CG_total counts the run's own iterations)
+        assert wa[k] == wb[k]
