@@ -203,3 +203,38 @@ def test_cli_stop_restart_is_bitwise(cli, tmp_path):
     wa, wb = (whole / "STOPPED.txt").read_text().splitlines(), (second / "STOPPED.txt").read_text().splitlines()
     for k in (1, 2, 4):  # time, step, rejected (CG_total counts the run's own iterations)
         assert wa[k] == wb[k]
+
+
+EXAMPLES = json.loads((GOLDEN / "examples_golden.json").read_text()) if (GOLDEN / "examples_golden.json").exists() else {}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(EXAMPLES))
+def test_cli_reference_examples(cli, tmp_path, name):
+    """Every example input shipped with the reference, 300 steps, against the
+    reference program's own run (make_examples_golden.py): same files, status
+    and step decisions; fields within the FP64 tolerances."""
+    from golden.make_cli_golden import read_container
+
+    ref = EXAMPLES[name]
+    lines = [(k, v) for k, v in ref["input"]]
+    p, out = _run(cli, lines, ["--max-steps", "300"], tmp_path, name)
+    assert p.returncode == ref["rc"]
+    assert p.stderr == ref["stderr"]
+    if ref["rc"]:
+        return
+    assert sorted(x.name for x in out.iterdir()) == ref["files"]
+    assert (out / ref["status_file"]).read_text() == ref["status"]
+    head, rows = _csv((out / "diagnostics.csv").read_text())
+    rhead, rrows = _csv(ref["diagnostics"])
+    assert head == rhead and len(rows) == len(rrows)
+    for r, g in zip(rows, rrows):
+        for k in ("time", "step", "dt_next", "cg_last", "cg_peak", "rejected", "shift_distance"):
+            assert r[k] == g[k], k
+    fields = read_container(out / "checkpoint.h5")
+    ref_fields = np.load(GOLDEN / "examples_fields.npz")
+    for a in ("alpha", "theta", "gamma"):
+        assert np.abs(fields[a] - ref_fields[f"{name}/{a}"]).max() <= 1e-10
+    assert np.abs(fields["mu"] - ref_fields[f"{name}/mu"]).max() <= 1e-5
+    c, c_ref = fields["carbon"], ref_fields[f"{name}/carbon"]
+    assert abs(c.sum() - c_ref.sum()) <= 1e-12 * abs(c_ref.sum())
