@@ -623,7 +623,10 @@ def adjoint_arm(args, rank: int, world: int, dist) -> None:
                "cpu": _cpu_model()}
     ctx.close()
     if rank == 0:
-        per_step = 2 * (80.0 + 64.0 * rep.cg_forward / K) + 48.0 + 160.0 + 64.0 * rep.cg_adjoint / K
+        # forward, recomputation of every segment but the last, tape, adjoint
+        nseg = -(-K // every)
+        recomputed = (nseg - 1) / nseg
+        per_step = (1.0 + recomputed) * (80.0 + 64.0 * rep.cg_forward / K) + 48.0 + 160.0 + 64.0 * rep.cg_adjoint / K
         algo = per_step * cell_steps
         peak, peak_kind = measured_peak()
         line = {
@@ -636,13 +639,15 @@ def adjoint_arm(args, rank: int, world: int, dist) -> None:
                        "objective": rep.objective, "gradient": list(rep.grad),
                        "fd_rel_err": fd_err, "cg_forward": rep.cg_forward, "cg_adjoint": rep.cg_adjoint,
                        "forward_ms": rep.forward_ms, "recompute_ms": rep.recompute_ms,
-                       "adjoint_ms": rep.adjoint_ms, "l2": "state 5 MB, tape 300 MB per segment",
+                       "adjoint_ms": rep.adjoint_ms,
+                       "l2": f"state {40 * w.cells / 1e6:.0f} MB, tape {48 * w.cells * min(K, every) / 1e6:.0f} MB",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": algo / (dev_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": algo / (dev_ms / 1e3) / 1e9 / peak, "traffic": None,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_kernel (forward, recompute with tape) + pearl_adjoint_kernel",
-                         "bytes_per_cell_step": "2*(80+64*n_CG) + 48 tape + 160 adjoint + 64*n_CG_adjoint"},
+                         "bytes_per_cell_step": "(1 + recomputed fraction)*(80+64*n_CG) + 48 tape + 160 adjoint "
+                                                "+ 64*n_CG_adjoint"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "gradient cell-steps/s", "h2d_bytes_per_step": 48 * w.cells / K,
                     "d2h_bytes_per_step": 40 * w.cells / K,
