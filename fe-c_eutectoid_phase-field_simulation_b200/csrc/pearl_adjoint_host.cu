@@ -20,6 +20,7 @@ using namespace pearl_gpu;
 namespace {
 
 int launch_adjoint(pearl_gpu_ctx* ctx, AdjArgs& args) {
+    const NvtxRange range(args.mode == 0 ? "pearl_gpu adjoint seed" : "pearl_gpu adjoint segment");
     if (!ctx->adj_grid) {
         int per_sm = 0, sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

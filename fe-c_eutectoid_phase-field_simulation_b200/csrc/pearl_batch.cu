@@ -112,6 +112,7 @@ int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma, int wx) {
 }
 
 int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
+    const NvtxRange range("pearl_gpu batch run");
     PB_CUDA(b, cudaSetDevice(b->device));
     PB_CUDA(b, cudaMemsetAsync(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups, b->stream));
     BatchArgs args{};

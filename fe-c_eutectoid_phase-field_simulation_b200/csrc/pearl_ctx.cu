@@ -173,6 +173,11 @@ int push_ctl(pearl_gpu_ctx* ctx) {
 // Launch the persistent kernel in `mode`; on return h_ctl holds the device
 // control block.  Maps the device status to the reference's messages.
 int launch(pearl_gpu_ctx* ctx, KArgs& args) {
+    static const char* const kNames[] = {"pearl_gpu run",       "pearl_gpu propose",  "pearl_gpu mixture",
+                                         "pearl_gpu diffusion", "pearl_gpu energy",   "pearl_gpu valid_state",
+                                         "pearl_gpu snapshot",  "pearl_gpu shift",    "pearl_gpu smooth",
+                                         "pearl_gpu mixture sums", "pearl_gpu init composition"};
+    const NvtxRange range(args.mode >= 0 && args.mode <= kModeInitComposition ? kNames[args.mode] : "pearl_gpu");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
     ctx->h_ctl->status = 0;
     ctx->h_ctl->why = 0;
@@ -320,6 +325,7 @@ int stage_grid(const pearl_gpu_ctx* ctx) {
 }
 
 int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* carbon, const double* mu) {
+    const NvtxRange range("pearl_gpu upload");
     if (int rc = ensure_stage(ctx)) return rc;
     const size_t n = (size_t)ctx->nx * ctx->ny;
     double* st = ctx->d_stage;
@@ -337,6 +343,7 @@ int upload_set(pearl_gpu_ctx* ctx, int set, const double* phi, const double* car
 }
 
 int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, double* mu) {
+    const NvtxRange range("pearl_gpu download");
     if (int rc = ensure_stage(ctx)) return rc;
     const size_t n = (size_t)ctx->nx * ctx->ny;
     double* st = ctx->d_stage;
@@ -465,6 +472,7 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->d_hist) cudaFree(ctx->d_hist);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     delete ctx;
@@ -534,7 +542,13 @@ int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_
     KArgs a{};
     a.mode = kModeRun;
     a.L = *limits;
+    if (ctx->d_hist) {
+        a.hist = ctx->d_hist;
+        a.hist_cap = ctx->hist_cap;
+        a.hist_next = ctx->hist_count % ctx->hist_cap;
+    }
     int rc = launch(ctx, a);
+    if (ctx->d_hist) ctx->hist_count += ctx->h_ctl->steps;
     if (report) {
         report->steps = ctx->h_ctl->steps;
         report->cg_total = ctx->h_ctl->cg_total;
@@ -543,6 +557,37 @@ int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_
         report->last = ctx->h_ctl->last;
     }
     return rc;
+}
+
+int pearl_gpu_set_history(pearl_gpu_ctx* ctx, long long capacity) {
+    if (!ctx || capacity < 0) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid history capacity");
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->d_hist) cudaFree(ctx->d_hist);
+    ctx->d_hist = nullptr;
+    ctx->hist_cap = 0;
+    ctx->hist_count = 0;
+    if (capacity == 0) return PEARL_OK;
+    PG_CUDA(ctx, cudaMalloc(&ctx->d_hist, sizeof(pearl_step_info) * (size_t)capacity));
+    ctx->hist_cap = capacity;
+    return PEARL_OK;
+}
+
+int pearl_gpu_get_history(pearl_gpu_ctx* ctx, pearl_step_info* out, long long max_entries, long long* returned,
+                          long long* recorded) {
+    if (!ctx || max_entries < 0 || (max_entries > 0 && !out)) return PEARL_ERR_INVALID_ARGUMENT;
+    const long long held = std::min(ctx->hist_count, ctx->hist_cap);
+    const long long n = std::min(held, max_entries);
+    // the last n entries, oldest first
+    for (long long k = 0; k < n; ++k) {
+        const long long idx = (ctx->hist_count - n + k) % ctx->hist_cap;
+        PG_CUDA(ctx, cudaMemcpyAsync(out + k, ctx->d_hist + idx, sizeof(pearl_step_info), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    }
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (returned) *returned = n;
+    if (recorded) *recorded = ctx->hist_count;
+    return PEARL_OK;
 }
 
 int pearl_gpu_advance(pearl_gpu_ctx* ctx, double stop_time, pearl_step_info* out) {

@@ -1558,6 +1558,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
             if (args.forced_dt) st.S.dt = args.forced_dt[steps];
             if (!advance(a, red, st, args.L.stop_time, info)) break;
             if (args.dt_log && leader) args.dt_log[steps] = info.accepted_dt;
+            if (args.hist && leader) args.hist[(args.hist_next + steps) % args.hist_cap] = info;
             if (args.tape) record_tape(a, st.cur, args.tape + args.tape_slot * steps);
             ++steps;
             cg_total += info.cg_iterations;

@@ -4,9 +4,20 @@
 
 #include <cuda_runtime.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <string>
 
 #include "pearl_kernels.cuh"
+
+// NVTX range for a host-side call (launches, transfers): named spans on a
+// profiler timeline; inert when no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct pearl_gpu_ctx {
     CUtensorMap maps[pearl_gpu::kMapCount];
@@ -27,6 +38,8 @@ struct pearl_gpu_ctx {
     double last_ms = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int adj_grid = 0;  // cooperative grid of the adjoint kernel (0 until first use)
+    pearl_step_info* d_hist = nullptr;  // per-step history ring (pearl_gpu_set_history)
+    long long hist_cap = 0, hist_count = 0;
     std::string error;
 };
 

@@ -45,6 +45,10 @@ struct KArgs {
     double* dt_log;
     double* tape;
     size_t tape_slot;
+    // per-step history ring (null = off): step k of the launch goes to
+    // hist[(hist_next + k) % hist_cap]
+    pearl_step_info* hist;
+    long long hist_cap, hist_next;
 };
 
 // One instance of a batch: its tensor maps, parameters and buffers.

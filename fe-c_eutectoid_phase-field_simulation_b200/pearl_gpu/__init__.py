@@ -119,6 +119,7 @@ EXPORTS = [
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
     "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit", "pearl_gpu_batch_configure",
+    "pearl_gpu_set_history", "pearl_gpu_get_history",
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -173,6 +174,9 @@ def library(path: Path | None = None) -> C.CDLL:
     IP = C.POINTER(C.c_int)
     L.pearl_gpu_adjoint_gradient.argtypes = [V, C.c_longlong, C.c_int, DP, C.POINTER(PearlAdjointReport)]
     L.pearl_gpu_set_precision.argtypes = [V, C.c_int]
+    L.pearl_gpu_set_history.argtypes = [V, C.c_longlong]
+    LLP = C.POINTER(C.c_longlong)
+    L.pearl_gpu_get_history.argtypes = [V, C.POINTER(PearlStepInfo), C.c_longlong, LLP, LLP]
     L.pearl_gpu_selftest_wait_limit.argtypes = [V, C.POINTER(C.c_int), DP]
     L.pearl_gpu_batch_set_precision.argtypes = [V, C.c_int]
     L.pearl_gpu_batch_create.argtypes = [C.c_int, C.POINTER(PearlParams), IP, IP, C.c_int, C.c_int, C.POINTER(V)]
@@ -361,6 +365,18 @@ class Context:
         v = C.c_int()
         self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
         return bool(v.value)
+
+    def set_history(self, capacity: int) -> None:
+        """Record every accepted step's PearlStepInfo in a device ring of `capacity` entries."""
+        self._check(self.lib.pearl_gpu_set_history(self.h, capacity))
+
+    def history(self, max_entries: int | None = None):
+        """(entries oldest first, steps recorded since set_history)."""
+        n = max_entries if max_entries is not None else 1 << 20
+        buf = (PearlStepInfo * max(n, 1))()
+        got, rec = C.c_longlong(), C.c_longlong()
+        self._check(self.lib.pearl_gpu_get_history(self.h, buf, n, C.byref(got), C.byref(rec)))
+        return list(buf)[: got.value], rec.value
 
     def selftest_wait_limit(self):
         """(status, device ms) of a grid barrier that cannot complete (see pearl_gpu.h)."""

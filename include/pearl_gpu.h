@@ -166,6 +166,18 @@ int pearl_gpu_advance(pearl_gpu_ctx* ctx, double stop_time, pearl_step_info* out
  * termination on the GPU (main's loop body, pearl_serial.cpp:2296-2306). */
 int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_report* report);
 
+/* Per-step history: with capacity > 0 the run loop records every accepted
+ * step's pearl_step_info (accepted dt, retries, CG iterations, residual,
+ * closure, ...) in a device ring of `capacity` entries, written inside the
+ * persistent kernel (capacity 0 turns it off; each call restarts the count).
+ * pearl_gpu_get_history copies the last min(recorded, capacity, max_entries)
+ * entries, oldest first; *recorded receives the steps recorded since
+ * pearl_gpu_set_history.  The reference keeps no such history
+ * (VALIDATION.md:57-62); it is what replaying a run's dt sequence needs. */
+int pearl_gpu_set_history(pearl_gpu_ctx* ctx, long long capacity);
+int pearl_gpu_get_history(pearl_gpu_ctx* ctx, pearl_step_info* out, long long max_entries, long long* returned,
+                          long long* recorded);
+
 /* Moving window (maybe_shift + shift_rows, pearl_serial.cpp:2023-2071).
  * *rows receives the number of rows shifted (0 if the front is below trigger). */
 int pearl_gpu_maybe_shift(pearl_gpu_ctx* ctx, double shift_trigger, double shift_target, double shift_gamma_carbon,

@@ -236,3 +236,41 @@ def test_bounded_wait_reports_and_recovers(gpu_lib):
         want = ref.download()
     for a, b in zip(got[:3], want[:3]):
         assert np.array_equal(a, b)
+
+
+def test_step_history_ring_and_replay(gpu_lib, port):
+    """The device history of a multi-step launch equals the per-step infos of
+    single advances, keeps the last `capacity` steps in order, and its accepted
+    dt sequence lets the oracle replay the run."""
+    import pearl_gpu
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    w = workloads.scaled(96, 128, seed=7, undercooling=20.0, dt=4e-12, dt_max=8e-12, jitter=0.1, front_jitter=1,
+                         front=24.0)
+    n = 20
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as ref:
+        ref.upload(w.phi, w.carbon, w.mu, w.scalars)
+        infos = [ref.advance() for _ in range(n)]
+    fields = [f for f, _ in pearl_gpu.PearlStepInfo._fields_]
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as ctx:
+        ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
+        ctx.set_history(8)
+        ctx.run(7)
+        ctx.run(n - 7)
+        last8, recorded = ctx.history()
+        assert recorded == n and len(last8) == 8
+        for h, i in zip(last8, infos[-8:]):
+            assert all(getattr(h, f) == getattr(i, f) for f in fields)
+        ctx.set_history(64)
+        ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
+        ctx.run(n)
+        hist, recorded = ctx.history()
+        phi, c, mu, _ = ctx.download()
+    assert recorded == n and len(hist) == n
+    assert sum(h.retries for h in hist) >= 1
+    po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    so = pyoracle.scalars_from(w.scalars)
+    rc, why, done, _ = port.advance_n(w.params, po, co, muo, so, n, forced_dt=[h.accepted_dt for h in hist])
+    assert rc == 0 and done == n, why
+    assert np.abs(phi - po).max() <= 1e-10 and np.abs(mu - muo).max() <= 1e-5
