@@ -22,6 +22,14 @@ domain, including rejected attempts.  Metric: cell-updates/s = nx*ny*steps/time.
   cpu_baseline / --impl reference: the reference solver compiled from its own
            source (oracle/_ref), else the C restatement, on host cores.
 
+Other workloads (same JSON contract, not the default line):
+  --precision mixed     the same domain with FP32 propose forces
+  --workload sweep      256 independent instances in one batched launch, with
+                        the autotuner and an all-cores CPU baseline
+  --workload adjoint    gradient of a 256x512, --steps-step run w.r.t. mobility,
+                        sigma and D_gamma (--checkpoint-every K), checked against
+                        central differences and the CPU reference gradient
+
 Multi-GPU: the path does not shard (one resident domain per GPU), so N GPUs run
 N independent replicas ("scaling": "weak"); time is the max over ranks.
 """
