@@ -72,6 +72,8 @@ def parse_args(argv=None):
                          "instances in one batched persistent launch; adjoint: gradient of a 256x512, "
                          "1000-step run (--steps sets the step count of that run)")
     ap.add_argument("--checkpoint-every", type=int, default=50, help="adjoint: steps per checkpoint segment")
+    ap.add_argument("--cpu-gradient-steps", type=int, default=100,
+                    help="adjoint: steps of the run the CPU reference gradient covers (bounded CPU time)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="fp64 (default): the reference's arithmetic; mixed: FP32 propose forces")
     ap.add_argument("--instances", type=int, default=256, help="sweep: number of instances")
@@ -614,7 +616,7 @@ def adjoint_arm(args, rank: int, world: int, dist) -> None:
         from oracle import pyoracle
 
         port = pyoracle.port()
-        kp = min(K, 100)
+        kp = min(K, max(1, args.cpu_gradient_steps))
         phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
         s = pyoracle.scalars_from(w.scalars)
         tc = time.perf_counter()
