@@ -559,6 +559,40 @@ int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_
     return rc;
 }
 
+int pearl_gpu_run_replay(pearl_gpu_ctx* ctx, const double* accepted_dt, long long n, pearl_run_report* report) {
+    if (!ctx || !accepted_dt || n < 1) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid replay");
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    double* d_dt = nullptr;
+    PG_CUDA(ctx, cudaMalloc(&d_dt, sizeof(double) * (size_t)n));
+    int rc = PEARL_OK;
+    if (cudaMemcpyAsync(d_dt, accepted_dt, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream) !=
+        cudaSuccess)
+        rc = fail(ctx, PEARL_ERR_CUDA, "replay dt upload");
+    if (rc == PEARL_OK) {
+        KArgs a{};
+        a.mode = kModeRun;
+        a.L = pearl_run_limits{n, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
+        a.forced_dt = d_dt;
+        if (ctx->d_hist) {
+            a.hist = ctx->d_hist;
+            a.hist_cap = ctx->hist_cap;
+            a.hist_next = ctx->hist_count % ctx->hist_cap;
+        }
+        rc = launch(ctx, a);
+        if (ctx->d_hist) ctx->hist_count += ctx->h_ctl->steps;
+        if (report) {
+            report->steps = ctx->h_ctl->steps;
+            report->cg_total = ctx->h_ctl->cg_total;
+            report->cg_peak = ctx->h_ctl->cg_peak;
+            report->reached_stop = ctx->h_ctl->reached_stop;
+            report->last = ctx->h_ctl->last;
+        }
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_dt);
+    return rc;
+}
+
 int pearl_gpu_set_history(pearl_gpu_ctx* ctx, long long capacity) {
     if (!ctx || capacity < 0) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid history capacity");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));

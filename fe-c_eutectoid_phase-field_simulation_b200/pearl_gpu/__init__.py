@@ -119,7 +119,7 @@ EXPORTS = [
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
     "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit", "pearl_gpu_batch_configure",
-    "pearl_gpu_set_history", "pearl_gpu_get_history",
+    "pearl_gpu_set_history", "pearl_gpu_get_history", "pearl_gpu_run_replay",
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -175,6 +175,7 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_adjoint_gradient.argtypes = [V, C.c_longlong, C.c_int, DP, C.POINTER(PearlAdjointReport)]
     L.pearl_gpu_set_precision.argtypes = [V, C.c_int]
     L.pearl_gpu_set_history.argtypes = [V, C.c_longlong]
+    L.pearl_gpu_run_replay.argtypes = [V, DP, C.c_longlong, C.POINTER(PearlRunReport)]
     LLP = C.POINTER(C.c_longlong)
     L.pearl_gpu_get_history.argtypes = [V, C.POINTER(PearlStepInfo), C.c_longlong, LLP, LLP]
     L.pearl_gpu_selftest_wait_limit.argtypes = [V, C.POINTER(C.c_int), DP]
@@ -365,6 +366,13 @@ class Context:
         v = C.c_int()
         self._check(self.lib.pearl_gpu_valid_state(self.h, C.byref(v)))
         return bool(v.value)
+
+    def run_replay(self, accepted_dt) -> PearlRunReport:
+        """Steps whose first attempt uses accepted_dt[k] (an oracle-style replay)."""
+        dts = np.ascontiguousarray(accepted_dt, dtype=np.float64)
+        rep = PearlRunReport()
+        self._check(self.lib.pearl_gpu_run_replay(self.h, _p(dts), dts.size, C.byref(rep)))
+        return rep
 
     def set_history(self, capacity: int) -> None:
         """Record every accepted step's PearlStepInfo in a device ring of `capacity` entries."""

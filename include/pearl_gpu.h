@@ -166,6 +166,13 @@ int pearl_gpu_advance(pearl_gpu_ctx* ctx, double stop_time, pearl_step_info* out
  * termination on the GPU (main's loop body, pearl_serial.cpp:2296-2306). */
 int pearl_gpu_run(pearl_gpu_ctx* ctx, const pearl_run_limits* limits, pearl_run_report* report);
 
+/* Replays an accepted-dt sequence: n steps, step k attempted first with
+ * accepted_dt[k] (host array) — the oracle replay of the reference
+ * (advance with s.dt set to the accepted dt, pearl_serial.cpp:1120).  A step
+ * whose forced dt is rejected retries with halved dt as usual, so a run that
+ * cannot follow the sequence shows it in its time and rejection count. */
+int pearl_gpu_run_replay(pearl_gpu_ctx* ctx, const double* accepted_dt, long long n, pearl_run_report* report);
+
 /* Per-step history: with capacity > 0 the run loop records every accepted
  * step's pearl_step_info (accepted dt, retries, CG iterations, residual,
  * closure, ...) in a device ring of `capacity` entries, written inside the

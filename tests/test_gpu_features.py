@@ -274,3 +274,28 @@ def test_step_history_ring_and_replay(gpu_lib, port):
     rc, why, done, _ = port.advance_n(w.params, po, co, muo, so, n, forced_dt=[h.accepted_dt for h in hist])
     assert rc == 0 and done == n, why
     assert np.abs(phi - po).max() <= 1e-10 and np.abs(mu - muo).max() <= 1e-5
+
+
+def test_run_replay_reproduces_a_run(gpu_lib):
+    """Replaying a run's recorded accepted-dt sequence (rejections included in the
+    original) reproduces its fields bitwise with no rejected attempt."""
+    import pearl_gpu
+    from pearl_gpu import workloads
+
+    w = workloads.scaled(96, 128, seed=7, undercooling=20.0, dt=4e-12, dt_max=8e-12, jitter=0.1, front_jitter=1,
+                         front=24.0)
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as a:
+        a.upload(w.phi, w.carbon, w.mu, w.scalars)
+        a.set_history(64)
+        a.run(25)
+        hist, _ = a.history()
+        want = a.download()
+    assert sum(h.retries for h in hist) >= 1
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as b:
+        b.upload(w.phi, w.carbon, w.mu, w.scalars)
+        rep = b.run_replay([h.accepted_dt for h in hist])
+        got = b.download()
+    assert rep.steps == 25 and got[3].rejected == 0
+    assert got[3].time == want[3].time
+    for x, y in zip(got[:3], want[:3]):
+        assert np.array_equal(x, y)
