@@ -5,6 +5,7 @@ Records each input's key-value lines (comments dropped), the status file,
 diagnostics.csv and the final checkpoint fields.
 
     python tests/golden/make_examples_golden.py
+    python tests/golden/make_examples_golden.py --write-input NAME PATH   # one stored input back to a file
 """
 from __future__ import annotations
 
@@ -71,5 +72,14 @@ def main() -> None:
     np.savez_compressed(HERE / "examples_fields.npz", **fields)
 
 
+def write_input(name: str, path: str) -> None:
+    """Writes the stored key-values of example `name` as an input file."""
+    kv = json.loads((HERE / "examples_golden.json").read_text())[name]["input"]
+    Path(path).write_text("\n".join(k if v is None else f"{k} = {v}" for k, v in kv) + "\n")
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) == 4 and sys.argv[1] == "--write-input":
+        write_input(sys.argv[2], sys.argv[3])
+    else:
+        main()
