@@ -612,11 +612,15 @@ int pearl_gpu_get_history(pearl_gpu_ctx* ctx, pearl_step_info* out, long long ma
     if (!ctx || max_entries < 0 || (max_entries > 0 && !out)) return PEARL_ERR_INVALID_ARGUMENT;
     const long long held = std::min(ctx->hist_count, ctx->hist_cap);
     const long long n = std::min(held, max_entries);
-    // the last n entries, oldest first
-    for (long long k = 0; k < n; ++k) {
-        const long long idx = (ctx->hist_count - n + k) % ctx->hist_cap;
-        PG_CUDA(ctx, cudaMemcpyAsync(out + k, ctx->d_hist + idx, sizeof(pearl_step_info), cudaMemcpyDeviceToHost,
-                                     ctx->stream));
+    // the last n entries, oldest first: at most two contiguous pieces of the ring
+    if (n > 0) {
+        const long long first = (ctx->hist_count - n) % ctx->hist_cap;
+        const long long head = std::min(n, ctx->hist_cap - first);
+        PG_CUDA(ctx, cudaMemcpyAsync(out, ctx->d_hist + first, sizeof(pearl_step_info) * (size_t)head,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+        if (n > head)
+            PG_CUDA(ctx, cudaMemcpyAsync(out + head, ctx->d_hist, sizeof(pearl_step_info) * (size_t)(n - head),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
     }
     PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (returned) *returned = n;
