@@ -469,6 +469,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
     clocks = ClockSampler(local)
     barrier()
     l0 = b.stats()["launches"]
+    rej0 = [b.download(i)[3].rejected for i in range(len(ws))]
     clocks.start()
     t0 = time.perf_counter()
     reps, st = b.run(args.steps)
@@ -481,6 +482,8 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
         raise RuntimeError(f"sweep instance failed: {[pearl_gpu.STATUS.get(x, x) for x in st if x]}")
     steps = [r.steps for r in reps]
     cell_updates = float(sum(w.cells * n for w, n in zip(ws, steps)))
+    rejected = [b.download(i)[3].rejected - r0 for i, r0 in enumerate(rej0)]
+    rejected_cell_attempts = float(sum(w.cells * r for w, r in zip(ws, rejected)))
     value, t_max = replica_throughput(dist, cell_updates, kernel_ms / 1e3, "cuda")
     cg = sum(r.cg_total * w.cells for r, w in zip(reps, ws))
     algo_bytes = 80.0 * cell_updates + 64.0 * cg
@@ -526,7 +529,11 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_batch_kernel (persistent FP64 step, block groups)",
-                         "algorithmic_bytes_per_launch": algo_bytes},
+                         "algorithmic_bytes_per_launch": algo_bytes,
+                         "rejected_attempts": int(sum(rejected)),
+                         "cg_per_step": sum(r.cg_total for r in reps) / max(1, sum(steps)),
+                         "rejected_share_of_cell_attempts": rejected_cell_attempts
+                         / (rejected_cell_attempts + cell_updates)},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_cells / e2e_t, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
                     "d2h_bytes_per_step": state_bytes / args.steps,
