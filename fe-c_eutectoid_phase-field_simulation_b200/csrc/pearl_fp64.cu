@@ -16,8 +16,13 @@
 //
 // Thread mapping: a warp covers 32 consecutive x of two adjacent rows; the
 // eight warps of a block stack 16 rows.  The two cells of a thread share their
-// vertical neighbour loads, and every load of a streaming phase is issued
-// before its arithmetic, doubling the bytes in flight per thread.
+// vertical neighbour loads.  Each phase's input fields are staged per tile by
+// 2-D TMA copies into shared memory through an mbarrier pipeline (`sweep`).
+//
+// This file also holds the batched kernel (block groups running independent
+// instances), the self-test kernels, and, through pearl_adjoint.cuh, the
+// reverse-step kernel; the host side lives in pearl_ctx.cu, pearl_batch.cu,
+// pearl_adjoint_host.cu and pearl_noalloc.cu.
 #include <cuda_runtime.h>
 
 #include <algorithm>
