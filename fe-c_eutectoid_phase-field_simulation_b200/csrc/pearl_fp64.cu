@@ -406,7 +406,12 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
         const int bx = t % P.ntx, by = t / P.ntx;
         const int s = k % S;
         double* dst = pp.stage + (size_t)s * NF * kFieldStride;
-        fence_proxy_async();  // earlier plain stores (global, and the stage's patch) before these async reads/writes
+        // plain stores of the earlier passes (ordered by the grid barrier) before the
+        // async reads of this sweep, once per sweep: no value that a sweep stages
+        // and uses is changed by a plain store of the same sweep (a field written
+        // in a pass is either not staged in it, or read only at the cells that the
+        // reading block itself writes, after reading them)
+        if (k == 0) fence_proxy_async();
         // tile-only boxes start at the tile (x multiple of 32 doubles); halo boxes two cells left, one row up
         mbar_arrive_expect_tx(&pp.bar[s], NF * (kTileOnly ? kTileX * kTileRows * (uint32_t)sizeof(double) : kBoxBytes));
 #pragma unroll
@@ -440,6 +445,7 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
                 const int col = side == 0 ? 1 : P.nx - (bx * kTileX - 2);
                 st[f * kFieldStride + r * kBoxW + col] = planes[f][(size_t)y * P.pitch + (side == 0 ? P.nx - 1 : 0)];
             }
+            fence_proxy_async_shared();  // the patch's plain writes before the stage's next async refill
             __syncthreads();
         }
         const Pair c = pair_of(P, t);
