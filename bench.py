@@ -77,7 +77,8 @@ def parse_args(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="fp64 (default): the reference's arithmetic; mixed: FP32 propose forces")
     ap.add_argument("--instances", type=int, default=256, help="sweep: number of instances")
-    ap.add_argument("--group-blocks", type=int, default=0, help="sweep: blocks per instance group (0 = autotune)")
+    ap.add_argument("--group-blocks", type=int, default=0,
+                    help="sweep: blocks per instance group (0 = autotune, -1 = sized per instance)")
     return ap.parse_args(argv)
 
 
@@ -449,7 +450,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
     ws = workloads.sweep(args.instances, seed=rank)
     cells = sum(w.cells for w in ws)
     b = pearl_gpu.Batch([(w.params, w.nx, w.ny) for w in ws], device=local,
-                        group_blocks=max(args.group_blocks, 0))
+                        group_blocks=max(args.group_blocks, -1))
     b.set_precision(args.precision)
     pinned = []
     for i, w in enumerate(ws):
@@ -457,8 +458,8 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
         pinned.append(hp)
         b.upload(i, *hp, w.scalars)
     tuned = None
-    if args.group_blocks <= 0:
-        tuned = b.autotune(steps=2)
+    if args.group_blocks == 0:
+        tuned = b.autotune(steps=10)
     b.run(max(args.warmup, 1))
 
     def barrier():

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -24,9 +25,12 @@ struct pearl_gpu_batch {
     BatchInstance* d_inst = nullptr;
     int* d_order = nullptr;
     int* d_first = nullptr;
+    int* d_block_group = nullptr;
+    int* d_group_block0 = nullptr;
     Ctl* d_group_ctl = nullptr;
     double* d_group_part = nullptr;
-    int per_sm = 0, sms = 0, grid = 0, group_blocks = 0, ngroups = 0;
+    int per_sm = 0, sms = 0, grid = 0, group_blocks = 0, ngroups = 0;  // group_blocks -1: sized per instance
+    double pass_overhead_tiles = 4;  // sized groups: fixed cost of a pass, in tiles of one block
     bool use_tma = true;      // TMA staging in use (needs the 32x16 tile)
     bool tma_capable = true;  // tensor maps of every instance encoded and the shared memory granted
     int tile_wx = 0;          // tile shape of every instance: 2^tile_wx warps side by side in x
@@ -49,56 +53,143 @@ int bfail(pearl_gpu_batch* b, int status, const std::string& msg) {
         if (e_ != cudaSuccess) return bfail(b, PEARL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// Give every instance the tile shape `wx`, split the cooperative grid into
-// groups of `gb` blocks and hand out the instances longest-first to the
-// least-loaded group (cost ~ cells).  TMA staging needs the 32x16 tile.
+// Assignment of instances to groups.  A pass over an instance of T tiles on a
+// group of g blocks takes about `o + ceil(T/g)` tile times (o: the pass's
+// fixed cost, grid barrier and pipeline fill, in tiles of one block), and a
+// group runs its instances one after another.  Instances go longest first to
+// the group where they would finish earliest (groups of one size are
+// interchangeable, so a min-heap per size suffices).  Returns the longest
+// group time; fills lists[g] when lists is given.
+double earliest_finish(const std::vector<long long>& tiles, const std::vector<int>& sizes, double o,
+                       std::vector<std::vector<int>>* lists) {
+    using Slot = std::pair<double, int>;  // (time so far, group)
+    std::vector<int> distinct;
+    for (int g : sizes)
+        if (std::find(distinct.begin(), distinct.end(), g) == distinct.end()) distinct.push_back(g);
+    std::sort(distinct.begin(), distinct.end());
+    std::vector<std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>>> heaps(distinct.size());
+    for (int j = 0; j < (int)sizes.size(); ++j)
+        heaps[std::lower_bound(distinct.begin(), distinct.end(), sizes[j]) - distinct.begin()].push({0.0, j});
+    std::vector<int> idx(tiles.size());
+    for (int i = 0; i < (int)idx.size(); ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return tiles[x] > tiles[y]; });
+    if (lists) lists->assign(sizes.size(), {});
+    double longest = 0;
+    for (int i : idx) {
+        int best = -1;
+        double finish = 0;
+        for (size_t k = 0; k < distinct.size(); ++k) {
+            if (heaps[k].empty()) continue;
+            const double f = heaps[k].top().first + o + (double)((tiles[i] + distinct[k] - 1) / distinct[k]);
+            if (best < 0 || f < finish) {
+                best = (int)k;
+                finish = f;
+            }
+        }
+        const Slot top = heaps[best].top();
+        heaps[best].pop();
+        heaps[best].push({finish, top.second});
+        if (lists) (*lists)[top.second].push_back(i);
+        longest = std::max(longest, finish);
+    }
+    return longest;
+}
+
+// Group sizes for PEARL_BATCH_SIZED_GROUPS: compositions of groups of s, 2s
+// and 4s blocks (s = 1, 2, .., 16) filling the grid, each scored by
+// earliest_finish; the shortest wins.  Groups left without an instance are
+// dropped.  Returns the sizes and fills lists.
+std::vector<int> sized_groups(const std::vector<long long>& tiles, int max_grid, double o,
+                              std::vector<std::vector<int>>& lists) {
+    std::vector<int> best;
+    double best_t = 0;
+    for (int s = 1; s <= 16 && s <= max_grid; s *= 2) {
+        const int big = 4 * s, mid = 2 * s;
+        const int step_big = std::max(1, max_grid / big / 32), step_mid = std::max(1, max_grid / mid / 32);
+        for (int nb = 0; nb * big <= max_grid; nb += step_big)
+            for (int nm = 0; nb * big + nm * mid <= max_grid; nm += step_mid) {
+                const int ns = (max_grid - nb * big - nm * mid) / s;
+                std::vector<int> sizes;
+                sizes.insert(sizes.end(), nb, big);
+                sizes.insert(sizes.end(), nm, mid);
+                sizes.insert(sizes.end(), ns, s);
+                if (sizes.empty()) continue;
+                const double t = earliest_finish(tiles, sizes, o, nullptr);
+                if (best.empty() || t < best_t) {
+                    best_t = t;
+                    best = sizes;
+                }
+            }
+    }
+    std::vector<std::vector<int>> all;
+    earliest_finish(tiles, best, o, &all);
+    std::vector<int> sizes;
+    lists.clear();
+    for (size_t g = 0; g < best.size(); ++g)
+        if (!all[g].empty()) {
+            sizes.push_back(best[g]);
+            lists.push_back(all[g]);
+        }
+    return sizes;
+}
+
+// Give every instance the tile shape `wx` and split the cooperative grid into
+// groups, of `gb` blocks each or, for gb = PEARL_BATCH_SIZED_GROUPS, of the
+// sizes sized_groups picks, with instances assigned by earliest_finish.  Only
+// a group's size bears on an instance's arithmetic (which block owns which
+// tile), not which group it is in.  TMA staging needs the 32x16 tile.
 int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma, int wx) {
     const int max_grid = b->per_sm * b->sms;
-    if (gb < 1 || gb > max_grid) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid group size");
+    if (gb != PEARL_BATCH_SIZED_GROUPS && (gb < 1 || gb > max_grid))
+        return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid group size");
     if (wx < 0 || wx > 3) return bfail(b, PEARL_ERR_INVALID_ARGUMENT, "invalid tile shape");
     b->group_blocks = gb;
-    b->ngroups = max_grid / gb;
-    b->grid = b->ngroups * gb;
     b->tile_wx = wx;
     b->use_tma = use_tma && wx == 0 && b->tma_capable;
     for (auto* c : b->inst) set_tile_shape(c, wx);
-    std::vector<int> idx(b->n);
-    for (int i = 0; i < b->n; ++i) idx[i] = i;
-    std::sort(idx.begin(), idx.end(), [&](int x, int y) {
-        return (long long)b->inst[x]->nx * b->inst[x]->ny > (long long)b->inst[y]->nx * b->inst[y]->ny;
-    });
-    std::vector<double> load(b->ngroups, 0.0);
-    std::vector<std::vector<int>> lists(b->ngroups);
-    for (int i : idx) {
-        // a group's blocks share an instance's tiles: cost = cells / min(blocks, tiles)
-        const pearl_gpu_ctx* c = b->inst[i];
-        const double cells = (double)c->nx * c->ny;
-        const double cost = cells / std::max(1, std::min(gb, c->P.ntiles));
-        int best = 0;
-        for (int g = 1; g < b->ngroups; ++g)
-            if (load[g] < load[best]) best = g;
-        load[best] += cost;
-        lists[best].push_back(i);
+    std::vector<long long> tiles(b->n);
+    for (int i = 0; i < b->n; ++i) tiles[i] = b->inst[i]->P.ntiles;
+    std::vector<int> sizes;                // blocks of each group
+    std::vector<std::vector<int>> lists;  // instances of each group
+    if (gb == PEARL_BATCH_SIZED_GROUPS) {
+        sizes = sized_groups(tiles, max_grid, b->pass_overhead_tiles, lists);
+    } else {
+        sizes.assign(max_grid / gb, gb);
+        earliest_finish(tiles, sizes, b->pass_overhead_tiles, &lists);
     }
-    std::vector<int> order, first(1, 0);
+    b->ngroups = (int)sizes.size();
+    std::vector<int> order, first(1, 0), block_group, group_block0(1, 0);
     for (int g = 0; g < b->ngroups; ++g) {
         order.insert(order.end(), lists[g].begin(), lists[g].end());
         first.push_back((int)order.size());
+        block_group.insert(block_group.end(), sizes[g], g);
+        group_block0.push_back((int)block_group.size());
     }
+    b->grid = (int)block_group.size();
     cudaFree(b->d_order);
     cudaFree(b->d_first);
+    cudaFree(b->d_block_group);
+    cudaFree(b->d_group_block0);
     cudaFree(b->d_group_ctl);
     cudaFree(b->d_group_part);
     b->d_order = nullptr;
     b->d_first = nullptr;
+    b->d_block_group = nullptr;
+    b->d_group_block0 = nullptr;
     b->d_group_ctl = nullptr;
     b->d_group_part = nullptr;
     PB_CUDA(b, cudaMalloc(&b->d_order, sizeof(int) * std::max(1, b->n)));
     PB_CUDA(b, cudaMalloc(&b->d_first, sizeof(int) * first.size()));
+    PB_CUDA(b, cudaMalloc(&b->d_block_group, sizeof(int) * block_group.size()));
+    PB_CUDA(b, cudaMalloc(&b->d_group_block0, sizeof(int) * group_block0.size()));
     PB_CUDA(b, cudaMalloc(&b->d_group_ctl, sizeof(Ctl) * b->ngroups));
-    PB_CUDA(b, cudaMalloc(&b->d_group_part, sizeof(double) * (size_t)b->ngroups * 2 * gb * kMaxRed));
+    PB_CUDA(b, cudaMalloc(&b->d_group_part, sizeof(double) * (size_t)b->grid * 2 * kMaxRed));
     PB_CUDA(b, cudaMemcpy(b->d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
     PB_CUDA(b, cudaMemcpy(b->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+    PB_CUDA(b, cudaMemcpy(b->d_block_group, block_group.data(), sizeof(int) * block_group.size(),
+                          cudaMemcpyHostToDevice));
+    PB_CUDA(b, cudaMemcpy(b->d_group_block0, group_block0.data(), sizeof(int) * group_block0.size(),
+                          cudaMemcpyHostToDevice));
     PB_CUDA(b, cudaMemset(b->d_group_ctl, 0, sizeof(Ctl) * b->ngroups));
     // per-instance descriptors (tensor maps, parameters, buffers)
     std::vector<BatchInstance> hi(b->n);
@@ -119,7 +210,8 @@ int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
     args.inst = b->d_inst;
     args.order = b->d_order;
     args.first = b->d_first;
-    args.group_blocks = b->group_blocks;
+    args.block_group = b->d_block_group;
+    args.group_block0 = b->d_group_block0;
     args.group_ctl = b->d_group_ctl;
     args.group_part = b->d_group_part;
     args.use_tma = b->use_tma ? 1 : 0;
@@ -156,6 +248,8 @@ void pearl_gpu_batch_destroy(pearl_gpu_batch* b) {
     cudaFree(b->d_inst);
     cudaFree(b->d_order);
     cudaFree(b->d_first);
+    cudaFree(b->d_block_group);
+    cudaFree(b->d_group_block0);
     cudaFree(b->d_group_ctl);
     cudaFree(b->d_group_part);
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -205,7 +299,8 @@ int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, con
         b->per_sm < 1)
         return bail(PEARL_ERR_CUDA);
     b->tma_capable = tma;
-    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : 4, tma, 0);
+    const int rc =
+        batch_configure(b, group_blocks > 0 || group_blocks == PEARL_BATCH_SIZED_GROUPS ? group_blocks : 4, tma, 0);
     if (rc) return bail(rc);
     *out = b;
     return PEARL_OK;
@@ -272,8 +367,18 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
     double best_ms = 1e300;
     int best_gb = b->group_blocks, best_wx = b->tile_wx;
     bool best_tma = b->use_tma;
-    const int cands[] = {1, 2, 4, 8, 16};
-    pearl_run_limits L{1, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
+    double best_o = b->pass_overhead_tiles;
+    // equal groups of 1..16 blocks, and groups sized per instance with three
+    // weights of a pass's fixed cost (in tiles of one block)
+    struct Cand {
+        int gb;
+        double o;
+    };
+    const Cand cands[] = {{1, 0},  {2, 0},  {4, 0},  {8, 0},  {16, 0}, {PEARL_BATCH_SIZED_GROUPS, 1},
+                          {PEARL_BATCH_SIZED_GROUPS, 4}, {PEARL_BATCH_SIZED_GROUPS, 16}};
+    // one launch of `steps` steps per trial: the first steps of a run carry the
+    // step-start energy and most rejected attempts, so single steps rank poorly
+    pearl_run_limits L{steps, 0x7fffffffffffffffLL, 1e300, 1e300, 0};
     // tile shapes 32x16 (with and without TMA staging), 64x8 and 128x4
     struct Shape {
         int wx;
@@ -286,13 +391,15 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
     shapes.push_back({2, false});
     for (const Shape& sh : shapes) {
         const int tma = sh.tma ? 1 : 0;
-        for (int gb : cands) {
+        for (const Cand& cand : cands) {
+            const int gb = cand.gb;
             if (gb > b->per_sm * b->sms) continue;
+            if (gb == PEARL_BATCH_SIZED_GROUPS) b->pass_overhead_tiles = cand.o;
             int rc = batch_configure(b, gb, tma != 0, sh.wx);
             double ms = 0;
-            for (int s = 0; rc == PEARL_OK && s < steps; ++s) {
+            if (rc == PEARL_OK) {
                 rc = batch_launch(b, L);
-                ms += b->last_ms;
+                ms = b->last_ms;
             }
             // restore
             for (int i = 0; i < b->n; ++i) {
@@ -313,10 +420,12 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
                 best_gb = gb;
                 best_tma = tma != 0;
                 best_wx = sh.wx;
+                if (gb == PEARL_BATCH_SIZED_GROUPS) best_o = cand.o;
             }
         }
     }
     release();
+    b->pass_overhead_tiles = best_o;
     const int rc = batch_configure(b, best_gb, best_tma, best_wx);
     if (group_blocks) *group_blocks = best_gb;
     if (use_tma) *use_tma = best_tma ? 1 : 0;

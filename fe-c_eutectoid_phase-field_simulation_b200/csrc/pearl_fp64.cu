@@ -1706,12 +1706,13 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
 // ------------------------------------------------------------------ batched instances
 // A batch advances many independent instances (own grid size, parameters,
 // dt, retries and CG count) in one cooperative launch.  The grid is split
-// into groups of `group_blocks` blocks; each group runs the same `advance`
-// device code on its own list of instances, one after another, with barriers
-// and reductions local to the group.
+// into groups of consecutive blocks (of equal or of per-instance sizes); each
+// group runs the same `advance` device code on its own list of instances, one
+// after another, with barriers and reductions local to the group.
 
 __global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
-    const int g = blockIdx.x / args.group_blocks, bid = blockIdx.x % args.group_blocks;
+    const int g = args.block_group[blockIdx.x];
+    const int b0 = args.group_block0[g], nblk = args.group_block0[g + 1] - b0, bid = (int)blockIdx.x - b0;
     __shared__ PhaseClock clk;
     __shared__ DevParams sP;
     __shared__ DevBufs sB;
@@ -1725,7 +1726,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_c
         __syncthreads();
     }
     Ctl* gctl = args.group_ctl + g;
-    double* gpart = args.group_part + (size_t)g * 2 * args.group_blocks * kMaxRed;
+    double* gpart = args.group_part + (size_t)b0 * 2 * kMaxRed;
     const bool leader = bid == 0 && threadIdx.x == 0;
     for (int j = args.first[g]; j < args.first[g + 1]; ++j) {
         const BatchInstance* I = args.inst + args.order[j];
@@ -1735,7 +1736,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_c
             sB = I->B;
         }
         __syncthreads();
-        const Dom a{sP, sB, I->maps, args.use_tma, bid, args.group_blocks, gctl, gpart, 0, 0, 0, 0, 0, 0, 0};
+        const Dom a{sP, sB, I->maps, args.use_tma, bid, nblk, gctl, gpart, 0, 0, 0, 0, 0, 0, 0};
         Red red(a, &clk);
         red.pipe_ptr = &pipe;
         Ctl* ctl = sB.ctl;

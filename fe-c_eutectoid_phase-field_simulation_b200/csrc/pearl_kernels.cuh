@@ -62,9 +62,10 @@ struct BatchArgs {
     const BatchInstance* inst;
     const int* order;  // instance ids grouped by block group
     const int* first;  // group g owns order[first[g] .. first[g+1])
-    int group_blocks;
-    Ctl* group_ctl;      // [groups] barrier words and error status
-    double* group_part;  // [groups][2][group_blocks][kMaxRed]
+    const int* block_group;   // [grid] group of each block
+    const int* group_block0;  // [groups + 1] group g owns blocks group_block0[g] .. group_block0[g+1]-1
+    Ctl* group_ctl;           // [groups] barrier words and error status
+    double* group_part;       // [grid][2][kMaxRed]: group g's slots start at block group_block0[g]
     int use_tma;
     pearl_run_limits L;
 };

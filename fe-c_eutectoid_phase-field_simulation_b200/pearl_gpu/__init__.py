@@ -123,6 +123,8 @@ EXPORTS = [
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
+# Batch group_blocks value for groups sized per instance (PEARL_BATCH_SIZED_GROUPS)
+BATCH_SIZED_GROUPS = -1
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
           "mixture", "shift", "snapshot", "smooth", "init", "adjoint"]

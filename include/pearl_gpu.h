@@ -310,13 +310,19 @@ int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, int checkpo
  * cooperative launch.  The grid is split into groups of `group_blocks`
  * blocks, each group with its own grid barrier and reduction slots; the
  * instances are assigned to groups longest-first, and a group runs its
- * instances one after another.  Every instance follows exactly the path of a
+ * instances one after another.  With group_blocks = PEARL_BATCH_SIZED_GROUPS
+ * the groups have per-instance sizes instead: each instance gets the smallest
+ * power-of-two group (1..64 blocks) that keeps the slowest group short, small
+ * instances share single-block groups, and spare blocks enlarge the slowest
+ * groups.  Every instance follows exactly the path of a
  * pearl_gpu_ctx (same kernels, same reduction order for the same group size),
  * so it is main's loop (pearl_serial.cpp:2296-2306) run once per instance.
  * No counterpart in the reference, which runs one case per process. */
 typedef struct pearl_gpu_batch pearl_gpu_batch;
+enum { PEARL_BATCH_SIZED_GROUPS = -1 };
 
-/* group_blocks <= 0 picks 4; pearl_gpu_batch_autotune can choose instead. */
+/* group_blocks: blocks per group, PEARL_BATCH_SIZED_GROUPS, or any other
+ * value <= 0 for 4; pearl_gpu_batch_autotune can choose instead. */
 int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, const int* ny, int device,
                            int group_blocks, pearl_gpu_batch** out);
 void pearl_gpu_batch_destroy(pearl_gpu_batch* batch);
@@ -331,8 +337,9 @@ int pearl_gpu_batch_download(pearl_gpu_batch* batch, int i, double* phi_aos3, do
  * PEARL_OK unless the launch itself failed. */
 int pearl_gpu_batch_run(pearl_gpu_batch* batch, const pearl_run_limits* limits, pearl_run_report* reports,
                         int* status);
-/* Times `steps` one-step launches for each group size in {1,2,4,8,16} and
- * each tile shape (32x16 cells with and without TMA staging, 64x8, 128x4),
+/* Times one launch of `steps` steps for each group size in {1,2,4,8,16}, for
+ * per-instance group sizes (three weights of a pass's fixed cost against its
+ * tiles), and each tile shape (32x16 cells with and without TMA staging, 64x8, 128x4),
  * restoring every instance's state after each trial, and keeps the fastest;
  * the choice is written to the out pointers (may be NULL; tile_warps_x = warps
  * side by side in x: 1, 2 or 4).  The tile shape changes which block owns
@@ -342,8 +349,10 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* batch, int steps, int* group_block
 /* pearl_gpu_set_precision for every instance. */
 int pearl_gpu_batch_set_precision(pearl_gpu_batch* batch, int precision);
 /* Sets the configuration pearl_gpu_batch_autotune would choose: blocks per
- * group, TMA staging (used only with tile_warps_x = 1) and the tile shape
- * (tile_warps_x warps side by side in x: 1, 2, 4 or 8). */
+ * group (or PEARL_BATCH_SIZED_GROUPS, with the fixed-cost weight the last
+ * autotune chose, initially 4 tiles), TMA staging (used only with
+ * tile_warps_x = 1) and the tile shape (tile_warps_x warps side by side in x:
+ * 1, 2, 4 or 8). */
 int pearl_gpu_batch_configure(pearl_gpu_batch* batch, int group_blocks, int use_tma, int tile_warps_x);
 int pearl_gpu_batch_stats(const pearl_gpu_batch* batch, long long* kernel_launches, int* grid_blocks,
                           int* group_blocks, double* last_kernel_ms);

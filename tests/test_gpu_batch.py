@@ -9,6 +9,9 @@ persistent launch, each following the single-domain step path.
     instances are then held to the FP64 bars against the oracle (max|dphi| <=
     1e-10, max|dmu| <= 1e-5 J/mol, total carbon 1e-12 relative) with the same
     accepted steps, retries and CG iteration counts.
+  * Groups sized per instance (PEARL_BATCH_SIZED_GROUPS) follow the same two
+    rules: small instances get a group with at least one block per tile when
+    the grid allows it, large ones fewer.
 """
 from __future__ import annotations
 
@@ -62,7 +65,7 @@ def test_batch_bitwise_equals_single_domains(gpu_lib):
         assert g[3].time == want[3].time and g[3].dt == want[3].dt and g[3].rejected == want[3].rejected
 
 
-@pytest.mark.parametrize("group_blocks", [1, 3])
+@pytest.mark.parametrize("group_blocks", [1, 3, -1])
 def test_batch_matches_oracle(gpu_lib, port, group_blocks):
     from oracle import pyoracle
 
@@ -125,7 +128,7 @@ def test_batch_autotune_keeps_state(gpu_lib):
     ws = _cases()
     with _batch(ws, 4) as a:
         gb, tma, wx = a.autotune(steps=1)
-        assert gb in (1, 2, 4, 8, 16) and wx in (1, 2, 4)
+        assert gb in (1, 2, 4, 8, 16, -1) and wx in (1, 2, 4)
         assert a.stats()["group_blocks"] == gb
         assert a.run(10)[1] == [0] * len(ws)
         fa = [a.download(i) for i in range(len(ws))]
@@ -157,6 +160,52 @@ def test_batch_tile_shapes_match_oracle(gpu_lib, port, wx):
         rc, why, done, _ = port.advance_n(w.params, phi_o, c_o, mu_o, so, n)
         assert rc == 0 and done == n, why
         assert s.rejected == so.rejected and s.step == so.step
+        assert np.abs(phi - phi_o).max() <= PHI_TOL
+        assert np.abs(mu - mu_o).max() <= MU_TOL
+        assert abs(c.sum() - c_o.sum()) <= MASS_RTOL * abs(c_o.sum())
+
+
+def test_batch_sized_groups(gpu_lib, port):
+    """Per-instance group sizes.  The small instances alone (6 to 10 tiles each)
+    get a group with a block per tile and equal their single-domain runs
+    bitwise.  Beside three 384x384 instances (288 tiles each, more than the
+    grid holds for them) every instance shares blocks between tiles and all
+    meet the FP64 bars against the oracle."""
+    import pearl_gpu
+    from pearl_gpu import workloads
+    from oracle import pyoracle
+
+    small = _cases()
+    n = 8
+    with _batch(small, pearl_gpu.BATCH_SIZED_GROUPS) as b:
+        assert b.stats()["group_blocks"] == pearl_gpu.BATCH_SIZED_GROUPS
+        reps, st = b.run(n)
+        assert st == [0] * len(small)
+        got = [b.download(i) for i in range(len(small))]
+    for w, rep, g in zip(small, reps, got):
+        with pearl_gpu.Context(w.params, w.nx, w.ny) as ctx:
+            ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
+            r = ctx.run(n)
+            want = ctx.download()
+        assert rep.cg_total == r.cg_total
+        for x, y in zip(g[:3], want[:3]):
+            assert np.array_equal(x, y)
+
+    large = [workloads.scaled(384, 384, seed=10 + k, undercooling=15.0 + 5 * k, dt=4e-12, dt_max=8e-12,
+                              front=40.0, pairs=6) for k in range(3)]
+    ws = large + small
+    with _batch(ws, pearl_gpu.BATCH_SIZED_GROUPS) as b:
+        assert 0 < b.stats()["grid"] <= 2 * 148
+        reps, st = b.run(n)
+        assert st == [0] * len(ws)
+        got = [b.download(i) for i in range(len(ws))]
+    for w, rep, (phi, c, mu, s) in zip(ws, reps, got):
+        phi_o, c_o, mu_o = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+        so = pyoracle.scalars_from(w.scalars)
+        rc, why, done, oinfos = port.advance_n(w.params, phi_o, c_o, mu_o, so, n)
+        assert rc == 0 and done == n, why
+        assert rep.steps == n and rep.cg_total == sum(i.cg_iterations for i in oinfos)
+        assert s.rejected == so.rejected and s.time == so.time
         assert np.abs(phi - phi_o).max() <= PHI_TOL
         assert np.abs(mu - mu_o).max() <= MU_TOL
         assert abs(c.sum() - c_o.sum()) <= MASS_RTOL * abs(c_o.sum())
