@@ -95,6 +95,18 @@ double earliest_finish(const std::vector<long long>& tiles, const std::vector<in
     return longest;
 }
 
+// Longest modelled group time of a given assignment.
+double earliest_finish_on(const std::vector<long long>& tiles, const std::vector<int>& sizes,
+                          const std::vector<std::vector<int>>& lists, double o) {
+    double longest = 0;
+    for (size_t g = 0; g < sizes.size(); ++g) {
+        double t = 0;
+        for (int i : lists[g]) t += o + (double)((tiles[i] + sizes[g] - 1) / sizes[g]);
+        longest = std::max(longest, t);
+    }
+    return longest;
+}
+
 // Group sizes for PEARL_BATCH_SIZED_GROUPS: compositions of groups of s, 2s
 // and 4s blocks (s = 1, 2, .., 16) filling the grid, each scored by
 // earliest_finish; the shortest wins.  Groups left without an instance are
@@ -133,6 +145,19 @@ std::vector<int> sized_groups(const std::vector<long long>& tiles, int max_grid,
     return sizes;
 }
 
+// The groups of a launch of `max_grid` blocks: gb blocks each, or the sizes
+// sized_groups picks for gb = PEARL_BATCH_SIZED_GROUPS, instances assigned by
+// earliest_finish.  Returns the modelled longest group time.
+double plan_groups(const std::vector<long long>& tiles, int max_grid, int gb, double o, std::vector<int>& sizes,
+                   std::vector<std::vector<int>>& lists) {
+    if (gb == PEARL_BATCH_SIZED_GROUPS) {
+        sizes = sized_groups(tiles, max_grid, o, lists);
+        return earliest_finish_on(tiles, sizes, lists, o);
+    }
+    sizes.assign(max_grid / gb, gb);
+    return earliest_finish(tiles, sizes, o, &lists);
+}
+
 // Give every instance the tile shape `wx` and split the cooperative grid into
 // groups, of `gb` blocks each or, for gb = PEARL_BATCH_SIZED_GROUPS, of the
 // sizes sized_groups picks, with instances assigned by earliest_finish.  Only
@@ -151,12 +176,7 @@ int batch_configure(pearl_gpu_batch* b, int gb, bool use_tma, int wx) {
     for (int i = 0; i < b->n; ++i) tiles[i] = b->inst[i]->P.ntiles;
     std::vector<int> sizes;                // blocks of each group
     std::vector<std::vector<int>> lists;  // instances of each group
-    if (gb == PEARL_BATCH_SIZED_GROUPS) {
-        sizes = sized_groups(tiles, max_grid, b->pass_overhead_tiles, lists);
-    } else {
-        sizes.assign(max_grid / gb, gb);
-        earliest_finish(tiles, sizes, b->pass_overhead_tiles, &lists);
-    }
+    plan_groups(tiles, max_grid, gb, b->pass_overhead_tiles, sizes, lists);
     b->ngroups = (int)sizes.size();
     std::vector<int> order, first(1, 0), block_group, group_block0(1, 0);
     for (int g = 0; g < b->ngroups; ++g) {
@@ -431,6 +451,28 @@ int pearl_gpu_batch_autotune(pearl_gpu_batch* b, int steps, int* group_blocks, i
     if (use_tma) *use_tma = best_tma ? 1 : 0;
     if (tile_warps_x) *tile_warps_x = 1 << best_wx;
     return rc;
+}
+
+int pearl_gpu_batch_plan(int n, const long long* tiles, int grid_blocks, int group_blocks, double pass_overhead_tiles,
+                         int* group_of_instance, int* group_size, int* ngroups, double* longest) {
+    if (n < 1 || !tiles || grid_blocks < 1 || !(pass_overhead_tiles >= 0) || !group_of_instance || !group_size ||
+        !ngroups)
+        return PEARL_ERR_INVALID_ARGUMENT;
+    if (group_blocks != PEARL_BATCH_SIZED_GROUPS && (group_blocks < 1 || group_blocks > grid_blocks))
+        return PEARL_ERR_INVALID_ARGUMENT;
+    std::vector<long long> t(tiles, tiles + n);
+    for (long long x : t)
+        if (x < 1) return PEARL_ERR_INVALID_ARGUMENT;
+    std::vector<int> sizes;
+    std::vector<std::vector<int>> lists;
+    const double m = plan_groups(t, grid_blocks, group_blocks, pass_overhead_tiles, sizes, lists);
+    for (size_t g = 0; g < sizes.size(); ++g) {
+        group_size[g] = sizes[g];
+        for (int i : lists[g]) group_of_instance[i] = (int)g;
+    }
+    *ngroups = (int)sizes.size();
+    if (longest) *longest = m;
+    return PEARL_OK;
 }
 
 int pearl_gpu_batch_configure(pearl_gpu_batch* b, int group_blocks, int use_tma, int tile_warps_x) {

@@ -119,7 +119,7 @@ EXPORTS = [
     "pearl_gpu_batch_upload", "pearl_gpu_batch_download", "pearl_gpu_batch_run", "pearl_gpu_batch_autotune",
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
     "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit", "pearl_gpu_batch_configure",
-    "pearl_gpu_set_history", "pearl_gpu_get_history", "pearl_gpu_run_replay",
+    "pearl_gpu_set_history", "pearl_gpu_get_history", "pearl_gpu_run_replay", "pearl_gpu_batch_plan",
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -190,12 +190,29 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_batch_run.argtypes = [V, C.POINTER(PearlRunLimits), C.POINTER(PearlRunReport), IP]
     L.pearl_gpu_batch_autotune.argtypes = [V, C.c_int, IP, IP, IP]
     L.pearl_gpu_batch_configure.argtypes = [V, C.c_int, C.c_int, C.c_int]
+    L.pearl_gpu_batch_plan.argtypes = [C.c_int, LLP, C.c_int, C.c_int, C.c_double, IP, IP, IP, DP]
     L.pearl_gpu_batch_stats.argtypes = [V, C.POINTER(C.c_longlong), IP, IP, DP]
     L.pearl_gpu_batch_last_error.argtypes = [V]
     L.pearl_gpu_batch_last_error.restype = C.c_char_p
     if path is None:
         _lib = L
     return L
+
+
+def batch_plan(tiles, grid_blocks: int, group_blocks: int = BATCH_SIZED_GROUPS, pass_overhead_tiles: float = 4.0):
+    """The groups a batch launch would use (pearl_gpu_batch_plan; host only):
+    (group of each instance, size of each group, modelled longest group time)."""
+    L = library()
+    t = np.ascontiguousarray(tiles, dtype=np.int64)
+    goi = np.zeros(len(t), dtype=np.int32)
+    gsz = np.zeros(max(grid_blocks, 1), dtype=np.int32)
+    ng, longest = C.c_int(), C.c_double()
+    rc = L.pearl_gpu_batch_plan(len(t), t.ctypes.data_as(C.POINTER(C.c_longlong)), grid_blocks, group_blocks,
+                                pass_overhead_tiles, goi.ctypes.data_as(C.POINTER(C.c_int)),
+                                gsz.ctypes.data_as(C.POINTER(C.c_int)), C.byref(ng), C.byref(longest))
+    if rc:
+        raise PearlError(rc, f"pearl_gpu_batch_plan failed: {STATUS.get(rc, rc)}")
+    return goi, gsz[: ng.value].copy(), longest.value
 
 
 def selftest_division(a: np.ndarray, b: np.ndarray, device: int = 0) -> int:

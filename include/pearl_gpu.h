@@ -354,6 +354,15 @@ int pearl_gpu_batch_set_precision(pearl_gpu_batch* batch, int precision);
  * tile_warps_x = 1) and the tile shape (tile_warps_x warps side by side in x:
  * 1, 2, 4 or 8). */
 int pearl_gpu_batch_configure(pearl_gpu_batch* batch, int group_blocks, int use_tma, int tile_warps_x);
+/* Host only (no GPU needed): the groups a batch launch of grid_blocks blocks
+ * would use for instances of tiles[i] tiles each (32x16-cell tiles:
+ * ceil(nx/32) * ceil(ny/16)), for group_blocks blocks per group or
+ * PEARL_BATCH_SIZED_GROUPS, with a pass's fixed cost weighed as
+ * pass_overhead_tiles tiles of one block.  Writes the group of every instance,
+ * the size of every group (group_size needs room for grid_blocks entries), the
+ * number of groups and the modelled longest group time in tiles (may be NULL). */
+int pearl_gpu_batch_plan(int n, const long long* tiles, int grid_blocks, int group_blocks, double pass_overhead_tiles,
+                         int* group_of_instance, int* group_size, int* ngroups, double* longest);
 int pearl_gpu_batch_stats(const pearl_gpu_batch* batch, long long* kernel_launches, int* grid_blocks,
                           int* group_blocks, double* last_kernel_ms);
 const char* pearl_gpu_batch_last_error(const pearl_gpu_batch* batch);
