@@ -113,6 +113,32 @@ def measured_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+# Bytes each pass of the persistent step reads and writes per cell (float64):
+# PROPOSE phi x3 + mu in, trial phi x3, K, chi, c(mu_ref) out; SETUP K, mu, chi,
+# c(mu_ref), c in, faces x2, x, r, z, diag out; APPLY faces x2, z, chi (+ p_old
+# after the first iteration) in, p, Ap out; UPDATE x, p, r, Ap, diag in, x, r, z
+# out; FINAL faces x2, x, trial phi x3, c, chi, c(mu_ref) in, r, c, mu out.
+PHASE_BYTES = {"propose": 80, "setup": 88, "apply_first": 48, "apply": 56, "update": 64, "final": 96}
+
+
+def phase_hbm_fracs(phase_ms: dict, phase_n: dict, cells: int, peak_gbs: float) -> dict:
+    """Per phase: its bytes over its clocked time (the phase clock includes the
+    phase's closing reduction), as a fraction of the HBM peak.  An APPLY after
+    SETUP or RESET starts a solve and reads no previous direction."""
+    out = {}
+    for k in ("propose", "setup", "apply", "update", "final"):
+        ms, n = phase_ms.get(k, 0.0), phase_n.get(k, 0)
+        if not ms or not n:
+            continue
+        if k == "apply":
+            first = min(n, phase_n.get("setup", 0) + phase_n.get("reset", 0))
+            nbytes = cells * (first * PHASE_BYTES["apply_first"] + (n - first) * PHASE_BYTES["apply"])
+        else:
+            nbytes = cells * n * PHASE_BYTES[k]
+        out[k] = round(nbytes / (ms / 1e3) / 1e9 / peak_gbs, 4)
+    return out
+
+
 def ncu_traffic_per_cell():
     """DRAM bytes per cell-update of pearl_kernel from the committed ncu summary, or None."""
     p = ROOT / "profiles" / "pearl_kernel_fp64_plain_large.md"
@@ -387,7 +413,9 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_kernel (persistent FP64 step)",
                          "algorithmic_bytes_per_launch": algo_bytes, "cg_iterations": rep.cg_total,
-                         "rejected_attempts": rejected, "phase_ms": phase_ms, "phase_count": phase_n},
+                         "rejected_attempts": rejected, "phase_ms": phase_ms, "phase_count": phase_n,
+                         "phase_hbm_frac": phase_hbm_fracs(phase_ms, phase_n, w.cells, peak),
+                         "phase_bytes_per_cell": PHASE_BYTES},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_state / m,
                     "d2h_bytes_per_step": bytes_state / m,

@@ -8,6 +8,7 @@ import subprocess
 import sys
 from pathlib import Path
 
+import pytest
 import torch.multiprocessing as mp
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -56,3 +57,21 @@ def test_reference_arm_json_contract():
         assert key in line
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["cores"] == 1
+
+
+def test_phase_hbm_fracs():
+    """Per-phase fractions from the phase clock: the numbers of a measured
+    2048x4096 line (100 steps, 114 attempts, 484 CG passes)."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    ms = {"propose": 35.553, "setup": 17.785, "apply": 47.882, "update": 41.305, "final": 32.653}
+    n = {"propose": 114, "setup": 114, "apply": 484, "update": 484, "final": 114}
+    f = bench.phase_hbm_fracs(ms, n, 2048 * 4096, 6551.0)
+    assert set(f) == set(ms)
+    # UPDATE: 64 B x 8.39 M cells x 484 passes in 41.3 ms
+    assert f["update"] == pytest.approx(64 * 2048 * 4096 * 484 / 41.305e-3 / 1e9 / 6551.0, rel=1e-3)
+    # APPLY: 114 first passes of 48 B, 370 of 56 B
+    assert f["apply"] == pytest.approx((114 * 48 + 370 * 56) * 2048 * 4096 / 47.882e-3 / 1e9 / 6551.0, rel=1e-3)
+    assert 0.9 < f["update"] < 1.0 and 0.6 < f["apply"] < 0.8
+    assert bench.phase_hbm_fracs({}, {}, 1, 1.0) == {}
