@@ -319,8 +319,7 @@ int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, con
         b->per_sm < 1)
         return bail(PEARL_ERR_CUDA);
     b->tma_capable = tma;
-    const int rc =
-        batch_configure(b, group_blocks > 0 || group_blocks == PEARL_BATCH_SIZED_GROUPS ? group_blocks : 4, tma, 0);
+    const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : PEARL_BATCH_SIZED_GROUPS, tma, 0);
     if (rc) return bail(rc);
     *out = b;
     return PEARL_OK;

@@ -321,8 +321,9 @@ int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, int checkpo
 typedef struct pearl_gpu_batch pearl_gpu_batch;
 enum { PEARL_BATCH_SIZED_GROUPS = -1 };
 
-/* group_blocks: blocks per group, PEARL_BATCH_SIZED_GROUPS, or any other
- * value <= 0 for 4; pearl_gpu_batch_autotune can choose instead. */
+/* group_blocks: blocks per group, or any value <= 0 (PEARL_BATCH_SIZED_GROUPS
+ * among them) for groups sized per instance; pearl_gpu_batch_autotune can
+ * choose instead. */
 int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, const int* ny, int device,
                            int group_blocks, pearl_gpu_batch** out);
 void pearl_gpu_batch_destroy(pearl_gpu_batch* batch);
