@@ -108,14 +108,20 @@ double earliest_finish_on(const std::vector<long long>& tiles, const std::vector
 }
 
 // Group sizes for PEARL_BATCH_SIZED_GROUPS: compositions of groups of s, 2s
-// and 4s blocks (s = 1, 2, .., 16) filling the grid, each scored by
-// earliest_finish; the shortest wins.  Groups left without an instance are
-// dropped.  Returns the sizes and fills lists.
+// and 4s blocks (s = 1, 2, 4, .. up to the grid) filling the grid, and one
+// group of floor(grid / n) blocks per instance (for a single instance: the
+// whole grid), each scored by earliest_finish; the shortest wins.  Groups left
+// without an instance are dropped.  Returns the sizes and fills lists.
 std::vector<int> sized_groups(const std::vector<long long>& tiles, int max_grid, double o,
                               std::vector<std::vector<int>>& lists) {
     std::vector<int> best;
     double best_t = 0;
-    for (int s = 1; s <= 16 && s <= max_grid; s *= 2) {
+    const int n = (int)tiles.size();
+    if (n <= max_grid) {
+        best.assign(n, max_grid / n);
+        best_t = earliest_finish(tiles, best, o, nullptr);
+    }
+    for (int s = 1; s <= max_grid; s *= 2) {
         const int big = 4 * s, mid = 2 * s;
         const int step_big = std::max(1, max_grid / big / 32), step_mid = std::max(1, max_grid / mid / 32);
         for (int nb = 0; nb * big <= max_grid; nb += step_big)

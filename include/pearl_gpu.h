@@ -311,10 +311,10 @@ int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, int checkpo
  * blocks, each group with its own grid barrier and reduction slots; the
  * instances are assigned to groups longest-first, and a group runs its
  * instances one after another.  With group_blocks = PEARL_BATCH_SIZED_GROUPS
- * the groups have per-instance sizes instead: each instance gets the smallest
- * power-of-two group (1..64 blocks) that keeps the slowest group short, small
- * instances share single-block groups, and spare blocks enlarge the slowest
- * groups.  Every instance follows exactly the path of a
+ * the groups have per-instance sizes instead, chosen so that the slowest group
+ * finishes soonest under a model of a pass's cost (powers of two up to the
+ * grid, or an equal share of the grid per instance): small instances share
+ * groups of a few blocks, large ones get many.  Every instance follows exactly the path of a
  * pearl_gpu_ctx (same kernels, same reduction order for the same group size),
  * so it is main's loop (pearl_serial.cpp:2296-2306) run once per instance.
  * No counterpart in the reference, which runs one case per process. */

@@ -46,7 +46,7 @@ def test_sized_plan_on_the_sweep(gpu_lib):
         goi, gsz, longest = pearl_gpu.batch_plan(tiles, GRID, pearl_gpu.BATCH_SIZED_GROUPS, o)
         counts = _check(tiles, goi, gsz, GRID)
         assert (counts > 0).all()
-        assert set(np.unique(gsz)) <= {1, 2, 4, 8, 16, 32, 64}
+        assert all(g & (g - 1) == 0 or g == GRID // len(tiles) for g in gsz)
         assert longest == pytest.approx(_modelled(tiles, goi, gsz, o))
         # at least as balanced as equal groups of 4 under the same model
         _, _, equal4 = pearl_gpu.batch_plan(tiles, GRID, 4, o)
@@ -89,6 +89,18 @@ def test_large_instances_share_blocks(gpu_lib):
     _check(tiles, goi, gsz, GRID)
     assert all(gsz[goi[i]] < tiles[i] for i in range(3))
     assert len({goi[i] for i in range(3)}) == 3  # one large instance per group
+
+
+def test_few_large_instances_use_the_grid(gpu_lib):
+    """One instance gets the whole grid, like a context of its own; two large
+    ones split it."""
+    import pearl_gpu
+
+    big = _tiles(2048, 4096)
+    goi, gsz, _ = pearl_gpu.batch_plan([big], GRID, pearl_gpu.BATCH_SIZED_GROUPS, 4.0)
+    assert list(gsz) == [GRID] and goi[0] == 0
+    goi, gsz, _ = pearl_gpu.batch_plan([big, big], GRID, pearl_gpu.BATCH_SIZED_GROUPS, 4.0)
+    assert sorted(gsz) == [GRID // 2, GRID // 2] and goi[0] != goi[1]
 
 
 @pytest.mark.parametrize("args", [
