@@ -113,6 +113,10 @@ def measured_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+# B200 HBM3e specification (the measured copy bandwidth in MEASURED_PEAKS.json is
+# the roofline's denominator; the fraction of this figure is reported beside it)
+SPEC_HBM_GBS = 8000.0
+
 # Bytes each pass of the persistent step reads and writes per cell (float64):
 # PROPOSE phi x3 + mu in, trial phi x3, K, chi, c(mu_ref) out; SETUP K, mu, chi,
 # c(mu_ref), c in, faces x2, x, r, z, diag out; APPLY faces x2, z, chi (+ p_old
@@ -410,6 +414,7 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
             "data": "synthetic", "config": config_dict(w, args),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "spec_gbs": SPEC_HBM_GBS, "frac_of_spec": achieved / SPEC_HBM_GBS,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_kernel (persistent FP64 step)",
                          "algorithmic_bytes_per_launch": algo_bytes, "cg_iterations": rep.cg_total,
@@ -556,6 +561,7 @@ def sweep_arm(args, rank: int, world: int, dist) -> None:
                        "parallelism": f"replicas x{world}", "bytes_per_cell_update": "80 + 64*n_CG"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
+                         "spec_gbs": SPEC_HBM_GBS, "frac_of_spec": achieved / SPEC_HBM_GBS,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_batch_kernel (persistent FP64 step, block groups)",
                          "algorithmic_bytes_per_launch": algo_bytes,
@@ -690,6 +696,7 @@ def adjoint_arm(args, rank: int, world: int, dist) -> None:
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": algo / (dev_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": algo / (dev_ms / 1e3) / 1e9 / peak, "traffic": None,
+                         "spec_gbs": SPEC_HBM_GBS, "frac_of_spec": algo / (dev_ms / 1e3) / 1e9 / SPEC_HBM_GBS,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_kernel (forward, recompute with tape) + pearl_adjoint_kernel",
                          "bytes_per_cell_step": "(1 + recomputed fraction)*(80+64*n_CG) + 48 tape + 160 adjoint "
