@@ -378,17 +378,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // tensor map maps[k]; slots whose bit is set in `stencil` also get the
 // periodic x wrap patched from `planes`.  Returns false after a bounded wait
 // ran out (the status is recorded; in-flight copies are drained, bounded).
+// `reverse` walks the block's tiles from its last to its first: consecutive
+// passes that alternate direction begin where the previous pass ended, on
+// tiles whose planes are still in L2.  The direction is fixed per phase, so
+// a run's sums do not depend on how it is split into launches.
 template <int NF, bool kTileOnly = false, class Body>
 __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const double* const (&planes)[NF],
-                      unsigned stencil, Body&& body) {
+                      unsigned stencil, bool reverse, Body&& body) {
     const DevParams& P = a.P;
+    const int G = a.nblk;
+    const int nb = a.bid < P.ntiles ? (P.ntiles - 1 - a.bid) / G + 1 : 0;
+    const auto tile_of = [&](int k) { return a.bid + (reverse ? nb - 1 - k : k) * G; };
     if (!a.use_tma) {
-        FOR_TILES(P) {
-            const Pair c = pair_of(P, t);
+        for (int k = 0; k < nb; ++k) {
+            const Pair c = pair_of(P, tile_of(k));
             if (!c.v0) continue;
             GlobalSrc<NF> src;
 #pragma unroll
-            for (int k = 0; k < NF; ++k) src.f[k] = planes[k];
+            for (int f = 0; f < NF; ++f) src.f[f] = planes[f];
             src.c = c;
             body(src, c);
         }
@@ -398,11 +405,9 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
                           ? (int)(kPipeDoubles / ((size_t)NF * kFieldStride))
                           : kMaxStages;
     static_assert(S >= 2, "pipeline needs two stages");
-    const int G = a.nblk;
-    const int nb = a.bid < P.ntiles ? (P.ntiles - 1 - a.bid) / G + 1 : 0;
     const auto issue = [&](int k) {
         if (threadIdx.x != 0) return;
-        const int t = a.bid + k * G;
+        const int t = tile_of(k);
         const int bx = t % P.ntx, by = t / P.ntx;
         const int s = k % S;
         double* dst = pp.stage + (size_t)s * NF * kFieldStride;
@@ -431,7 +436,7 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
             return false;
         }
         pp.parity ^= 1u << s;
-        const int t = a.bid + k * G;
+        const int t = tile_of(k);
         const int bx = t % P.ntx, by = t / P.ntx;
         double* st = pp.stage + (size_t)s * NF * kFieldStride;
         const bool left = bx == 0, right = (bx + 1) * kTileX >= P.nx;
@@ -628,9 +633,9 @@ __device__ bool phase_propose(const Dom& a, Red& red, int cur, double dt, double
         }
     };
     const bool ok =
-        P.mixed ? sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u,
+        P.mixed ? sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, true,
                            [&](const auto& src, const Pair& c) { body(std::true_type{}, src, c); })
-                : sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u,
+                : sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, true,
                            [&](const auto& src, const Pair& c) { body(std::false_type{}, src, c); });
     if (!ok) return false;
     double v[3] = {vchange, vmix, vsimp};
@@ -673,7 +678,7 @@ __device__ bool phase_setup(const Dom& a, Red& red, int cur, double dt, double& 
     double s0 = 0, s1 = 0, s2 = 0;
     const int maps[5] = {kMapK, kMapState + 5 * cur + 4, kMapChi, kMapIcpt, kMapState + 5 * cur + 3};
     const double* const planes[5] = {B.K, B.mu[cur], B.chi, B.icpt, B.c[cur]};
-    const bool ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x3u, [&](const auto& src, const Pair& c) {
+    const bool ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x3u, false, [&](const auto& src, const Pair& c) {
         const S2 K = stencil2(src, 0, c.v1);
         S2 u = stencil2(src, 1, c.v1);
         u.c0 -= P.mu_ref; u.c1 -= P.mu_ref; u.w0 -= P.mu_ref; u.e0 -= P.mu_ref;
@@ -758,11 +763,11 @@ __device__ bool phase_apply(const Dom& a, Red& red, double dt, bool first, doubl
     if (first) {
         const int maps[4] = {kMapWE, kMapWN, kMapZ, kMapChi};
         const double* const planes[4] = {B.wE, B.wN, B.z, B.chi};
-        ok = sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, body);
+        ok = sweep<4>(a, *red.pipe_ptr, maps, planes, 0x7u, true, body);
     } else {
         const int maps[5] = {kMapWE, kMapWN, kMapZ, kMapChi, pout ? kMapP0 : kMapP1};
         const double* const planes[5] = {B.wE, B.wN, B.z, B.chi, B.p[pout ^ 1]};
-        ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x17u, body);
+        ok = sweep<5>(a, *red.pipe_ptr, maps, planes, 0x17u, true, body);
     }
     if (!ok) return false;
     double v[1] = {s};
@@ -778,7 +783,7 @@ __device__ bool phase_update(const Dom& a, Red& red, double alpha, int pcur, dou
     double s0 = 0, s1 = 0;
     const int maps[5] = {kMapXc, pcur ? kMapP1c : kMapP0c, kMapRc, kMapApc, kMapDiagc};
     const double* const planes[5] = {B.x, B.p[pcur], B.r, B.Ap, B.diag};
-    const bool ok = sweep<5, true>(a, *red.pipe_ptr, maps, planes, 0x0u, [&](const auto& src, const Pair& c) {
+    const bool ok = sweep<5, true>(a, *red.pipe_ptr, maps, planes, 0x0u, false, [&](const auto& src, const Pair& c) {
         {
             const double x = src.v(0, 0, kC) + alpha * src.v(1, 0, kC), r = src.v(2, 0, kC) - alpha * src.v(3, 0, kC);
             const double z = r / src.v(4, 0, kC);
@@ -846,7 +851,7 @@ __device__ bool phase_final(const Dom& a, Red& red, int cur, double dt, double& 
                          kMapState + 5 * cur + 3, kMapChi, kMapIcpt};
     const double* const planes[9] = {B.wE, B.wN, B.x, B.phi[tr][0], B.phi[tr][1], B.phi[tr][2], B.c[cur], B.chi,
                                      B.icpt};
-    const bool ok = sweep<9>(a, *red.pipe_ptr, maps, planes, 0x3Fu, [&](const auto& src, const Pair& c) {
+    const bool ok = sweep<9>(a, *red.pipe_ptr, maps, planes, 0x3Fu, true, [&](const auto& src, const Pair& c) {
 #pragma unroll 1
         for (int k = 0; k < 2; ++k) {
             if (k == 1 && !c.v1) break;
