@@ -372,7 +372,7 @@ __device__ bool adj_step(const Dom& a, Red& red, const AdjArgs& g, const double*
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads, 2) pearl_adjoint_kernel(const __grid_constant__ AdjArgs args) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_adjoint_kernel(const __grid_constant__ AdjArgs args) {
     const Dom a{args.P, args.B, nullptr, 0, (int)blockIdx.x, (int)gridDim.x, args.B.ctl, args.B.part,
                 0, 0, 0, 0, 0, 0, 0};
     __shared__ PhaseClock clk;

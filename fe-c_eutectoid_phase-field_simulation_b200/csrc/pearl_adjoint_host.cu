@@ -19,15 +19,18 @@ using namespace pearl_gpu;
 // ============================================================ adjoint
 namespace {
 
+// The adjoint kernel runs in 256-thread blocks, two per SM, for every context.
+constexpr int kAdjThreads = tile_geometry(8).threads;
+
 int launch_adjoint(pearl_gpu_ctx* ctx, AdjArgs& args) {
     const NvtxRange range(args.mode == 0 ? "pearl_gpu adjoint seed" : "pearl_gpu adjoint segment");
     if (!ctx->adj_grid) {
         int per_sm = 0, sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_adjoint_kernel, kThreads, 0));
+        PG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::pearl_adjoint_kernel, kAdjThreads, 0));
         if (per_sm < 1) return fail(ctx, PEARL_ERR_CUDA, "adjoint kernel cannot be resident");
         const long long cells = (long long)ctx->nx * ctx->ny;
-        const long long want = (cells + kThreads - 1) / kThreads;
+        const long long want = (cells + kAdjThreads - 1) / kAdjThreads;
         // the reduction partials of the context are sized for ctx->grid blocks
         ctx->adj_grid = (int)std::max(1LL, std::min<long long>({want, (long long)per_sm * sms, (long long)ctx->grid}));
     }
@@ -39,7 +42,7 @@ int launch_adjoint(pearl_gpu_ctx* ctx, AdjArgs& args) {
     args.P = ctx->P;
     args.B = ctx->B;
     void* kargs[] = {&args};
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_adjoint_kernel, dim3(ctx->adj_grid), dim3(kThreads),
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)g8::pearl_adjoint_kernel, dim3(ctx->adj_grid), dim3(kAdjThreads),
                                              kargs, 0, ctx->stream));
     ctx->launches++;
     rc = pull_ctl(ctx);

@@ -244,8 +244,9 @@ int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
     args.L = L;
     void* kargs[] = {&args};
     PB_CUDA(b, cudaEventRecord(b->ev0, b->stream));
-    PB_CUDA(b, cudaLaunchCooperativeKernel((const void*)pearl_batch_kernel, dim3(b->grid), dim3(kThreads), kargs,
-                                           b->use_tma ? kTmaSmemBytes : 0, b->stream));
+    constexpr TileGeometry g = tile_geometry(8);
+    PB_CUDA(b, cudaLaunchCooperativeKernel((const void*)g8::pearl_batch_kernel, dim3(b->grid), dim3(g.threads), kargs,
+                                           b->use_tma ? g.tma_smem_bytes : 0, b->stream));
     b->launches++;
     PB_CUDA(b, cudaEventRecord(b->ev1, b->stream));
     PB_CUDA(b, cudaMemcpyAsync(b->h_ctls, b->d_ctls, sizeof(Ctl) * b->n, cudaMemcpyDeviceToHost, b->stream));
@@ -306,6 +307,7 @@ int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, con
         const int rc = pearl_gpu_create(&params[i], nx[i], ny[i], device, &b->inst[i]);
         if (rc) return bail(rc);
         pearl_gpu_ctx* c = b->inst[i];
+        set_geometry(c, 8);  // the batch kernel runs 256-thread blocks, two per SM
         cudaFree(c->d_ctl);  // the batch keeps every control block in one array
         c->d_ctl = b->d_ctls + i;
         c->B.ctl = c->d_ctl;
@@ -317,11 +319,12 @@ int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, con
         return bail(PEARL_ERR_CUDA);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
     if (tma &&
-        cudaFuncSetAttribute(pearl_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
+        cudaFuncSetAttribute(g8::pearl_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tile_geometry(8).tma_smem_bytes) !=
             cudaSuccess)
         tma = false;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->per_sm, pearl_batch_kernel, kThreads,
-                                                      tma ? kTmaSmemBytes : 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->per_sm, g8::pearl_batch_kernel, tile_geometry(8).threads,
+                                                      tma ? tile_geometry(8).tma_smem_bytes : 0) != cudaSuccess ||
         b->per_sm < 1)
         return bail(PEARL_ERR_CUDA);
     b->tma_capable = tma;

@@ -63,14 +63,25 @@ double host_psi(const pearl_params* p, int a, double mu) {
     return std::fma(-0.25 / p->A[a], d * d, p->C[a]);
 }
 
-// Tile of (32 << wx) x (2 << (3 - wx)) cells: 2^wx warps side by side in x.
+// Tile of (32 << wx) x (2 warps >> wx) cells: 2^wx warps side by side in x.
 void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2) {
     DevParams& P = ctx->P;
     P.warps_x_log2 = wx_log2;
-    const int tile_w = 32 << wx_log2, tile_h = 2 << (3 - wx_log2);
+    const int tile_w = 32 << wx_log2, tile_h = tile_geometry(ctx->warps).rows >> wx_log2;
     P.ntx = (ctx->nx + tile_w - 1) / tile_w;
     P.nty = (ctx->ny + tile_h - 1) / tile_h;
     P.ntiles = P.ntx * P.nty;
+}
+
+const void* step_kernel(int warps) {
+    return warps == 16 ? (const void*)g16::pearl_kernel : (const void*)g8::pearl_kernel;
+}
+
+void set_geometry(pearl_gpu_ctx* ctx, int warps) {
+    if (ctx->warps == warps) return;
+    ctx->warps = warps;
+    set_tile_shape(ctx, ctx->P.warps_x_log2);
+    if (ctx->use_tma && !build_tensor_maps(ctx)) ctx->use_tma = false;
 }
 
 void fill_dev_params(pearl_gpu_ctx* ctx) {
@@ -190,9 +201,9 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
     PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     args.use_tma = ctx->use_tma ? 1 : 0;
     if (ctx->use_tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(ctx->grid), dim3(kThreads), kargs,
-                                             ctx->use_tma ? kTmaSmemBytes : 0,
-                                             ctx->stream));
+    const TileGeometry g = tile_geometry(ctx->warps);
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel(step_kernel(ctx->warps), dim3(ctx->grid), dim3(g.threads), kargs,
+                                             ctx->use_tma ? g.tma_smem_bytes : 0, ctx->stream));
     ctx->launches++;
     PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     rc = pull_ctl(ctx);
@@ -228,7 +239,7 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
 size_t plane_elems(const pearl_gpu_ctx* ctx) { return (size_t)ctx->pitch * ctx->ny; }
 
 // 2-D TMA descriptors for the planes the stencil phases stage through shared
-// memory: box (kBoxW x kBoxH) float64, dims (nx, ny), row stride pitch*8 bytes,
+// memory: box (kBoxW x box_h of the context's block shape) float64, dims (nx, ny), row stride pitch*8 bytes,
 // zero fill outside.  Returns false when the driver cannot encode them; the
 // kernels then read the planes directly.
 bool build_tensor_maps(pearl_gpu_ctx* ctx) {
@@ -270,7 +281,8 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
         const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
         const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(double)};
         const bool tile_only = m >= kMapXc;
-        const cuuint32_t box[2] = {(cuuint32_t)(tile_only ? kTileX : kBoxW), (cuuint32_t)(tile_only ? kTileRows : kBoxH)};
+        const TileGeometry g = tile_geometry(ctx->warps);
+        const cuuint32_t box[2] = {(cuuint32_t)(tile_only ? kTileX : kBoxW), (cuuint32_t)(tile_only ? g.rows : g.box_h)};
         const cuuint32_t estr[2] = {1, 1};
         if (encode(&ctx->maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, planes[m], dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -409,17 +421,26 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (!coop) return bail(PEARL_ERR_NO_DEVICE);
+    // Block shape: 16 warps (512 threads, one block per SM, 32x32 tiles) when the
+    // domain gives every SM at least four such tiles, 8 warps (two 256-thread
+    // blocks per SM, 32x16 tiles) for smaller domains, which need the finer
+    // split; PEARL_GPU_TILE_WARPS = 8 or 16 overrides.
+    {
+        const long long tiles16 = (long long)((nx + 31) / 32) * ((ny + 31) / 32);
+        ctx->warps = tiles16 >= 4LL * sms ? 16 : 8;
+        if (const char* e = std::getenv("PEARL_GPU_TILE_WARPS")) ctx->warps = std::atoi(e) == 16 ? 16 : 8;
+    }
     fill_dev_params(ctx);
     // TMA staging of the stencil phases needs the 32x16 tile; PEARL_GPU_TMA=0 turns it off.
     const char* tma_env = std::getenv("PEARL_GPU_TMA");
     ctx->use_tma = ctx->P.warps_x_log2 == 0 && !(tma_env && std::atoi(tma_env) == 0);
-    if (ctx->use_tma &&
-        cudaFuncSetAttribute(pearl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemBytes) !=
-            cudaSuccess)
+    const TileGeometry geom = tile_geometry(ctx->warps);
+    if (ctx->use_tma && cudaFuncSetAttribute(step_kernel(ctx->warps), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)geom.tma_smem_bytes) != cudaSuccess)
         ctx->use_tma = false;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads,
-                                                      ctx->use_tma ? kTmaSmemBytes : 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(ctx->warps), geom.threads,
+                                                      ctx->use_tma ? geom.tma_smem_bytes : 0) != cudaSuccess ||
         per_sm < 1)
         return bail(PEARL_ERR_CUDA);
     ctx->grid = std::max(1, std::min(per_sm * sms, ctx->P.ntiles));
@@ -814,7 +835,7 @@ int pearl_gpu_selftest_division(int device, const double* a, const double* b, lo
                            cudaMemset(dm, 0, sizeof(unsigned long long)) != cudaSuccess))
         rc = PEARL_ERR_CUDA;
     if (rc == PEARL_OK) {
-        division_selftest_kernel<<<1184, 256>>>(da, db, drb, n, dm, 1);
+        g8::division_selftest_kernel<<<1184, 256>>>(da, db, drb, n, dm, 1);
         if (cudaDeviceSynchronize() != cudaSuccess ||
             cudaMemcpy(mismatches, dm, sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
             rc = PEARL_ERR_CUDA;
@@ -837,8 +858,8 @@ int pearl_gpu_selftest_wait_limit(pearl_gpu_ctx* ctx, int* status, double* waite
     Ctl* ctl = ctx->d_ctl;
     void* kargs[] = {&ctl};
     PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)wait_limit_selftest_kernel, dim3(ctx->grid),
-                                             dim3(kThreads), kargs, 0, ctx->stream));
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)g8::wait_limit_selftest_kernel, dim3(ctx->grid),
+                                             dim3(tile_geometry(8).threads), kargs, 0, ctx->stream));
     ctx->launches++;
     PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     rc = pull_ctl(ctx);

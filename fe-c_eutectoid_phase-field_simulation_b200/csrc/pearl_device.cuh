@@ -17,10 +17,7 @@
 
 namespace pearl_gpu {
 
-constexpr int kTileX = 32;     // one warp spans 32 consecutive x cells (256 B of a row)
-constexpr int kTileY = 8;      // 8 warps per block
-constexpr int kTileRows = 16;  // each warp covers two adjacent rows
-constexpr int kThreads = kTileX * kTileY;
+constexpr int kTileX = 32;  // one warp spans 32 consecutive x cells (256 B of a row)
 constexpr int kMaxRed = 6;  // values per grid reduction
 
 // Device copy of pearl_params plus host-precomputed constants.  Each constant
@@ -204,15 +201,58 @@ __device__ __forceinline__ double local_tau(const DevParams& P, double p0, doubl
 // the periodic x wrap is patched with plain loads and the y walls never read
 // their ghost row (the zero-flux faces are skipped or weighted by zero).
 constexpr int kBoxW = kTileX + 4;
-constexpr int kBoxH = kTileRows + 2;
-constexpr uint32_t kBoxBytes = kBoxW * kBoxH * sizeof(double);        // 5184
-constexpr int kFieldStride = ((kBoxBytes + 127) / 128 * 128) / 8;     // doubles per staged field (128 B aligned)
 constexpr int kMaxStageFields = 9;
 constexpr int kMaxStages = 4;
-// Shared-memory budget of the pipeline: two stages of the widest phase (9 fields);
-// phases staging fewer fields run more stages in the same space (up to 4).
-constexpr size_t kPipeDoubles = (size_t)2 * kMaxStageFields * kFieldStride;
-constexpr size_t kTmaSmemBytes = 128 + kPipeDoubles * sizeof(double);
+
+// Block shape.  A block of `warps` warps covers a tile 32 cells wide and 2 x
+// warps rows high (each warp two adjacent rows).  The device code is compiled
+// for two shapes: 8 warps (256 threads, two blocks per SM: 32x16 tiles) and 16
+// warps (512 threads, one block per SM: 32x32 tiles, 148 blocks in the grid
+// barrier and 5% fewer halo bytes per tile), in namespaces g8 and g16.  The
+// shared-memory budget of the pipeline is two stages of the widest phase (9
+// fields); phases staging fewer fields run more stages in the same space (up to 4).
+struct TileGeometry {
+    int warps, threads, rows;  // warps per block, threads, tile height in cells
+    int box_h;                 // staged box height: the tile plus one halo row above and below
+    int field_stride;          // doubles per staged field (128 B aligned)
+    size_t pipe_doubles;       // pipeline stage buffers
+    size_t tma_smem_bytes;     // dynamic shared memory of a block with TMA staging
+    int min_blocks;            // resident blocks per SM the kernels are compiled for
+};
+constexpr TileGeometry tile_geometry(int warps) {
+    const int box_h = 2 * warps + 2;
+    const int stride = (int)(((size_t)kBoxW * box_h * sizeof(double) + 127) / 128 * 128 / sizeof(double));
+    const size_t pipe = (size_t)2 * kMaxStageFields * stride;
+    return TileGeometry{warps, 32 * warps, 2 * warps, box_h, stride, pipe, 128 + pipe * sizeof(double),
+                        warps >= 16 ? 1 : 2};
+}
+
+#ifndef PEARL_TILE_WARPS
+#define PEARL_TILE_WARPS 8
+#endif
+#if PEARL_TILE_WARPS == 16
+#define PEARL_GEOM_NS g16
+#elif PEARL_TILE_WARPS == 8
+#define PEARL_GEOM_NS g8
+#else
+#error "PEARL_TILE_WARPS must be 8 or 16"
+#endif
+
+// The block shape this translation unit's device code is compiled for.
+namespace PEARL_GEOM_NS {
+constexpr TileGeometry kGeom = tile_geometry(PEARL_TILE_WARPS);
+constexpr int kTileY = kGeom.warps;
+constexpr int kTileRows = kGeom.rows;
+constexpr int kTileRowsLog2 = kTileRows == 32 ? 5 : 4;
+static_assert((1 << kTileRowsLog2) == kTileRows, "tile height is a power of two");
+constexpr int kThreads = kGeom.threads;
+constexpr int kBoxH = kGeom.box_h;
+constexpr uint32_t kBoxBytes = kBoxW * kBoxH * sizeof(double);
+constexpr int kFieldStride = kGeom.field_stride;
+constexpr size_t kPipeDoubles = kGeom.pipe_doubles;
+constexpr size_t kTmaSmemBytes = kGeom.tma_smem_bytes;
+constexpr int kMinBlocks = kGeom.min_blocks;
+}  // namespace PEARL_GEOM_NS
 
 // Tensor-map slots: state set s fields 0..4 (phi_a, phi_t, phi_g, c, mu) at
 // 5*s + f, then the work planes.
@@ -317,6 +357,7 @@ __device__ __forceinline__ double red_identity(unsigned op) {
 }
 __device__ __forceinline__ unsigned op_of(unsigned ops, int k) { return (ops >> (2 * k)) & 3u; }
 
+namespace PEARL_GEOM_NS {  // the block's warps
 template <int NV>
 __device__ __forceinline__ void block_publish(const double (&v)[NV], unsigned ops, double* part_slot, int bid) {
     __shared__ double s_red[kThreads / 32][kMaxRed];
@@ -340,6 +381,7 @@ __device__ __forceinline__ void block_publish(const double (&v)[NV], unsigned op
         }
     }
 }
+}  // namespace PEARL_GEOM_NS
 
 template <int NV>
 __device__ __forceinline__ void grid_gather(double (&out)[NV], unsigned ops, const double* part_slot, int nblk) {

@@ -40,6 +40,7 @@
 #include "pearl_kernels.cuh"
 
 namespace pearl_gpu {
+namespace PEARL_GEOM_NS {  // compiled once per block shape (PEARL_TILE_WARPS = 8, 16)
 
 
 
@@ -73,11 +74,11 @@ struct Pair {
 __device__ __forceinline__ Pair pair_of(const DevParams& P, int t) {
     Pair c;
     const int bx = t % P.ntx, by = t / P.ntx;
-    // the 8 warps of a block are arranged 2^wx side by side in x and 8/2^wx in y
+    // the kTileY warps of a block are arranged 2^wx side by side in x and kTileY/2^wx in y
     const int warp = threadIdx.x >> 5;
     const int wx = warp & ((1 << P.warps_x_log2) - 1), wy = warp >> P.warps_x_log2;
     c.x = (bx << (5 + P.warps_x_log2)) + (wx << 5) + (threadIdx.x & 31);
-    c.y0 = (by << (4 - P.warps_x_log2)) + 2 * wy;
+    c.y0 = (by << (kTileRowsLog2 - P.warps_x_log2)) + 2 * wy;
     c.v0 = c.x < P.nx && c.y0 < P.ny;
     c.v1 = c.v0 && c.y0 + 1 < P.ny;
     const int xw = c.x == 0 ? P.nx - 1 : c.x - 1;
@@ -1534,7 +1535,7 @@ __device__ void record_tape(const Dom& a, int cur, double* slot) {
         for (int f = 0; f < 6; ++f) slot[f * pe + i] = src[f][i];
 }
 
-__global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs args) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __grid_constant__ KArgs args) {
     const Dom a{args.P, args.B, args.maps, args.use_tma, (int)blockIdx.x, (int)gridDim.x, args.B.ctl, args.B.part,
                 args.shift_trigger, args.shift_target, args.shift_c_gamma, args.smooth_max_steps,
                 args.smooth_min_steps, args.smooth_energy_rtol, args.smooth_max_phase_change};
@@ -1715,7 +1716,7 @@ __global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constan
 // group runs the same `advance` device code on its own list of instances, one
 // after another, with barriers and reductions local to the group.
 
-__global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
     const int g = args.block_group[blockIdx.x];
     const int b0 = args.group_block0[g], nblk = args.group_block0[g + 1] - b0, bid = (int)blockIdx.x - b0;
     __shared__ PhaseClock clk;
@@ -1824,5 +1825,6 @@ __global__ void wait_limit_selftest_kernel(Ctl* ctl) { grid_barrier(ctl, gridDim
 
 #include "pearl_adjoint.cuh"
 
+}  // namespace PEARL_GEOM_NS
 }  // namespace pearl_gpu
 

@@ -21,6 +21,7 @@ struct NvtxRange {
 
 struct pearl_gpu_ctx {
     CUtensorMap maps[pearl_gpu::kMapCount];
+    int warps = 8;  // block shape of the context's kernels: 8 or 16 warps (pearl_gpu::tile_geometry)
     bool use_tma = false;
     int device = 0;
     int nx = 0, ny = 0, pitch = 0;
@@ -52,8 +53,13 @@ int fail(pearl_gpu_ctx* ctx, int status, const std::string& msg);
 int cuda_fail(pearl_gpu_ctx* ctx, cudaError_t e, const char* what);
 bool valid_params(const pearl_params* p);
 double host_psi(const pearl_params* p, int a, double mu);
-// Tile of (32 << wx) x (2 << (3 - wx)) cells: 2^wx warps side by side in x.
+// Tile of (32 << wx) x (2 warps >> wx) cells: 2^wx warps side by side in x.
 void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2);
+// The persistent step kernel of a block shape.
+const void* step_kernel(int warps);
+// Gives the context the kernels of another block shape (tile counts and TMA
+// boxes follow); its own launch grid is kept.
+void set_geometry(pearl_gpu_ctx* ctx, int warps);
 void fill_dev_params(pearl_gpu_ctx* ctx);
 int pull_ctl(pearl_gpu_ctx* ctx);
 int push_ctl(pearl_gpu_ctx* ctx);

@@ -96,11 +96,24 @@ struct AdjArgs {
     double* acc;           // [0] objective, [1..3] gradient (M, sigma, D_gamma), [4] adjoint CG iterations
 };
 
-__global__ void __launch_bounds__(kThreads, 2) pearl_kernel(const __grid_constant__ KArgs args);
-__global__ void __launch_bounds__(kThreads, 2) pearl_batch_kernel(const __grid_constant__ BatchArgs args);
-__global__ void __launch_bounds__(kThreads, 2) pearl_adjoint_kernel(const __grid_constant__ AdjArgs args);
-__global__ void division_selftest_kernel(const double* a, const double* b, const double* rb, long long n,
-                                         unsigned long long* mismatches, int use_exact);
-__global__ void wait_limit_selftest_kernel(Ctl* ctl);
+// The kernels of each block shape (tile_geometry): g8 for 256-thread blocks,
+// two per SM; g16 for 512-thread blocks, one per SM.
+#define PEARL_DECLARE_KERNELS(WARPS, MIN_BLOCKS)                                                                \
+    __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS) pearl_kernel(const __grid_constant__ KArgs args); \
+    __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS)                                                 \
+        pearl_batch_kernel(const __grid_constant__ BatchArgs args);                                           \
+    __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS)                                                 \
+        pearl_adjoint_kernel(const __grid_constant__ AdjArgs args);                                           \
+    __global__ void division_selftest_kernel(const double* a, const double* b, const double* rb, long long n,  \
+                                             unsigned long long* mismatches, int use_exact);                  \
+    __global__ void wait_limit_selftest_kernel(Ctl* ctl);
+namespace g8 {
+PEARL_DECLARE_KERNELS(8, 2)
+}
+namespace g16 {
+PEARL_DECLARE_KERNELS(16, 1)
+}
+#undef PEARL_DECLARE_KERNELS
+static_assert(tile_geometry(8).min_blocks == 2 && tile_geometry(16).min_blocks == 1, "kernel launch bounds");
 
 }  // namespace pearl_gpu

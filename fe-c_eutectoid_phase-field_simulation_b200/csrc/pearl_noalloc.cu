@@ -108,7 +108,8 @@ extern "C" int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int
 
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pearl_kernel, kThreads, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, g8::pearl_kernel, tile_geometry(8).threads, 0) !=
+            cudaSuccess ||
         per_sm < 1)
         return PEARL_ERR_CUDA;
     const int grid = std::max(1, std::min(std::min(per_sm * sms, ctx.P.ntiles), kNoAllocMaxBlocks));
@@ -132,7 +133,8 @@ extern "C" int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int
     a.L.end_time = INFINITY;
     a.L.output_eps = 0;
     void* kargs[] = {&a};
-    if (cudaLaunchCooperativeKernel((const void*)pearl_kernel, dim3(grid), dim3(kThreads), kargs, 0, st) !=
+    if (cudaLaunchCooperativeKernel((const void*)g8::pearl_kernel, dim3(grid), dim3(tile_geometry(8).threads), kargs, 0,
+                                    st) !=
         cudaSuccess)
         return PEARL_ERR_CUDA;
     if (cudaMemcpyAsync(&h, B.ctl, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -24,13 +24,16 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 # FP64 path: -fmad=false keeps every multiply and add separately rounded, as in
 # the reference built for plain x86-64, so per-cell results match bitwise.
-CU_SOURCES = {
-    "pearl_fp64.cu": ["-fmad=false"],        # phases and kernels
-    "pearl_ctx.cu": ["-fmad=false"],         # context, transfers, single-domain C ABI
-    "pearl_batch.cu": ["-fmad=false"],       # batched instances
-    "pearl_adjoint_host.cu": ["-fmad=false"],  # adjoint gradient driver
-    "pearl_noalloc.cu": ["-fmad=false"],     # step without device allocation
-}
+# (object, source, flags); the phases and kernels are compiled once per block
+# shape: 8 warps (namespace g8) and 16 warps (namespace g16).
+CU_SOURCES = [
+    ("pearl_fp64_g8", "pearl_fp64.cu", ["-fmad=false", "-DPEARL_TILE_WARPS=8"]),    # phases and kernels
+    ("pearl_fp64_g16", "pearl_fp64.cu", ["-fmad=false", "-DPEARL_TILE_WARPS=16"]),
+    ("pearl_ctx", "pearl_ctx.cu", ["-fmad=false"]),            # context, transfers, single-domain C ABI
+    ("pearl_batch", "pearl_batch.cu", ["-fmad=false"]),        # batched instances
+    ("pearl_adjoint_host", "pearl_adjoint_host.cu", ["-fmad=false"]),  # adjoint gradient driver
+    ("pearl_noalloc", "pearl_noalloc.cu", ["-fmad=false"]),    # step without device allocation
+]
 # host driver (the pearl_gpu executable): C++17, linked against libpearl_gpu.so
 CLI_SOURCES = ["config.cpp", "io.cpp", "main.cpp"]
 
@@ -57,8 +60,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     deps = sources() + [Path(__file__)]
     if force or _newer(LIB, deps):
         objs = []
-        for name, extra in CU_SOURCES.items():
-            obj = BUILD / (Path(name).stem + ".o")
+        for stem, name, extra in CU_SOURCES:
+            obj = BUILD / (stem + ".o")
             cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", *extra, "-Xcompiler", "-fPIC",
                    f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / name), "-o", str(obj)]
             if verbose:
