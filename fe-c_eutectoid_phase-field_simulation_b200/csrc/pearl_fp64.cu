@@ -3,7 +3,7 @@
 // including the retry loop and the Jacobi-PCG solve, with every decision
 // (dt, acceptance, CG termination) taken on the device.
 //
-// Phases of one attempt (each is a sweep over 32x16-cell tiles followed by a
+// Phases of one attempt (each is a sweep over the block's tiles followed by a
 // deterministic grid reduction and a bounded grid barrier):
 //   PROPOSE  propose_phi (:961-1002) + mixture of the trial phi (:1013-1020)
 //   SETUP    implicit_diffusion set-up: apply(mu_offset), r, z, diag (:1021-1046)
@@ -15,9 +15,12 @@
 //   RESET    z = r/diag ; <r,z> when the true residual misses     (:1060-1064)
 //
 // Thread mapping: a warp covers 32 consecutive x of two adjacent rows; the
-// eight warps of a block stack 16 rows.  The two cells of a thread share their
-// vertical neighbour loads.  Each phase's input fields are staged per tile by
-// 2-D TMA copies into shared memory through an mbarrier pipeline (`sweep`).
+// kTileY warps of a block stack 2 x kTileY rows.  This file is compiled once
+// per block shape (PEARL_TILE_WARPS = 8: 32x16 tiles, two 256-thread blocks
+// per SM; 16: 32x32 tiles, one 512-thread block per SM), into namespaces g8
+// and g16.  The two cells of a thread share their vertical neighbour loads.
+// Each phase's input fields are staged per tile by 2-D TMA copies into shared
+// memory through an mbarrier pipeline (`sweep`).
 //
 // This file also holds the batched kernel (block groups running independent
 // instances), the self-test kernels, and, through pearl_adjoint.cuh, the
