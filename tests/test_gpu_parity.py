@@ -198,3 +198,32 @@ def test_full_size_large_workload_replay(gpu_lib, port):
     assert np.abs(phi - po).max() <= PHI_TOL
     assert np.abs(mu - muo).max() <= MU_TOL
     assert abs(c.sum() - co.sum()) <= MASS_RTOL * abs(co.sum())
+
+
+@pytest.mark.parametrize("warps", [8, 16])
+def test_block_shapes_match_oracle(gpu_lib, port, monkeypatch, warps):
+    """Both block shapes (256-thread blocks with 32x16 tiles, 512-thread blocks
+    with 32x32 tiles; a 1024x1024 domain takes the latter by default) against
+    the oracle on the same domain: the shape changes only which block owns
+    which cells, so the steps, rejections and CG counts agree and the fields
+    meet the FP64 bars."""
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    monkeypatch.setenv("PEARL_GPU_TILE_WARPS", str(warps))
+    w = workloads.scaled(1024, 1024, seed=21, undercooling=20.0, dt=4e-12, dt_max=8e-12, front=48.0, pairs=32,
+                         jitter=0.1)
+    n = 6
+    with _ctx(w) as ctx:
+        infos = [ctx.advance() for _ in range(n)]
+        phi, c, mu, s = ctx.download()
+    po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    so = pyoracle.scalars_from(w.scalars)
+    rc, why, done, oinfos = port.advance_n(w.params, po, co, muo, so, n)
+    assert rc == 0 and done == n, why
+    assert [i.cg_iterations for i in infos] == [i.cg_iterations for i in oinfos]
+    assert [i.retries for i in infos] == [i.retries for i in oinfos]
+    assert s.time == so.time and s.rejected == so.rejected
+    assert np.abs(phi - po).max() <= PHI_TOL
+    assert np.abs(mu - muo).max() <= MU_TOL
+    assert abs(c.sum() - co.sum()) <= MASS_RTOL * abs(co.sum())
