@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent.parent  # fe-c_eutectoid_phase-field_simulation_b200/
@@ -59,15 +60,19 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     deps = sources() + [Path(__file__)]
     if force or _newer(LIB, deps):
-        objs = []
+        objs, cmds = [], []
         for stem, name, extra in CU_SOURCES:
             obj = BUILD / (stem + ".o")
             cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", *extra, "-Xcompiler", "-fPIC",
                    f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(CSRC / name), "-o", str(obj)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
-            _run(cmd)
+            cmds.append(cmd)
             objs.append(obj)
+        # the translation units are independent: compile them side by side
+        with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+            for f in [pool.submit(_run, c) for c in cmds]:
+                f.result()
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(LIB)])
     if force or _newer(CLI, deps + [LIB]):
         # -ffp-contract=off: host arithmetic that mirrors the reference (temperature
