@@ -417,6 +417,8 @@ def gpu_arm(args, rank: int, world: int, dist) -> None:
                          "spec_gbs": SPEC_HBM_GBS, "frac_of_spec": achieved / SPEC_HBM_GBS,
                          "peak_source": f"{peak_kind} HBM copy bandwidth",
                          "kernel": "pearl_kernel (persistent FP64 step)",
+                         # 148 on B200: one 512-thread block per SM (32x32 tiles); 296: two 256-thread blocks
+                         "grid_blocks": ctx.stats()["grid"],
                          "algorithmic_bytes_per_launch": algo_bytes, "cg_iterations": rep.cg_total,
                          "rejected_attempts": rejected, "phase_ms": phase_ms, "phase_count": phase_n,
                          "phase_hbm_frac": phase_hbm_fracs(phase_ms, phase_n, w.cells, peak),
