@@ -30,6 +30,9 @@ Other workloads (same JSON contract, not the default line):
                         sigma and D_gamma (--checkpoint-every K), checked against
                         central differences and the CPU reference gradient
 
+Profiling aids (no bench line): --probe propose | diffusion launches one phase
+of the step on its own; --probe fp64-peak measures the FP64 roofline.
+
 Multi-GPU: the path does not shard (one resident domain per GPU), so N GPUs run
 N independent replicas ("scaling": "weak"); time is the max over ranks.
 """
@@ -76,6 +79,10 @@ def parse_args(argv=None):
                     help="adjoint: steps of the run the CPU reference gradient covers (bounded CPU time)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="fp64 (default): the reference's arithmetic; mixed: FP32 propose forces")
+    ap.add_argument("--probe", choices=["propose", "diffusion", "fp64-peak"], default=None,
+                    help="profiling aid instead of the bench line: launch one phase of the hot path on its own "
+                         "(propose: propose_phi + mixture; diffusion: one proposal, then the implicit solve) "
+                         "--steps times on the --nx x --ny large workload, or measure the FP64 peak")
     ap.add_argument("--instances", type=int, default=256, help="sweep: number of instances")
     ap.add_argument("--group-blocks", type=int, default=0,
                     help="sweep: blocks per instance group (0 = autotune, -1 = sized per instance)")
@@ -713,8 +720,38 @@ def adjoint_arm(args, rank: int, world: int, dist) -> None:
         print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ single-phase probes
+def probe_arm(args) -> None:
+    """One phase of the time step as its own launch, so that a profiler sees it
+    alone (the step itself is one persistent kernel), or the FP64 peak of the
+    device.  Prints one JSON line per launch; not a bench line."""
+    import pearl_gpu
+
+    if args.probe == "fp64-peak":
+        print(json.dumps({"probe": "fp64-peak", "fp64_tflops": pearl_gpu.fp64_peak_tflops(0)}), flush=True)
+        return
+    w = workload(args.nx, args.ny)
+    dt = w.meta["dt"]
+    with pearl_gpu.Context(w.params, w.nx, w.ny) as ctx:
+        ctx.set_precision(args.precision)
+        ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
+        for _ in range(max(1, args.steps)):
+            if args.probe == "propose":
+                change = ctx.propose_phi(dt)
+                out = {"probe": "propose", "max_phase_change": change}
+            else:
+                ctx.propose_phi(dt)
+                d = ctx.implicit_diffusion(dt)
+                out = {"probe": "diffusion", "ok": d["ok"], "cg_iterations": d["it"]}
+            out.update(nx=w.nx, ny=w.ny, precision=args.precision, kernel_ms=ctx.stats()["last_ms"])
+            print(json.dumps(out), flush=True)
+
+
 def main(argv=None) -> int:
     args = parse_args(argv)
+    if args.probe:
+        probe_arm(args)
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

@@ -374,6 +374,18 @@ int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, doubl
 
 }  // namespace pearl_gpu
 
+// FP64 throughput probe: eight independent FMA chains per thread, so the FP64
+// pipe, not the dependency latency, bounds the loop.
+__global__ void fp64_fma_chains_kernel(double* out, int iters, double a, double b) {
+    double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
+           x7 = x0 + 7;
+    for (int i = 0; i < iters; ++i) {
+        x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+        x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
 extern "C" {
 
 const char* pearl_gpu_status_string(int status) {
@@ -844,6 +856,41 @@ int pearl_gpu_selftest_division(int device, const double* a, const double* b, lo
     cudaFree(db);
     cudaFree(drb);
     cudaFree(dm);
+    return rc;
+}
+
+int pearl_gpu_selftest_fp64_peak(int device, double* tflops) {
+    if (!tflops) return PEARL_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return PEARL_ERR_NO_DEVICE;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms < 1)
+        return PEARL_ERR_CUDA;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    double* out = nullptr;
+    if (cudaMalloc(&out, sizeof(double) * blocks * threads) != cudaSuccess) return PEARL_ERR_CUDA;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = PEARL_OK;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = PEARL_ERR_CUDA;
+    double best = 0;
+    if (rc == PEARL_OK) {
+        fp64_fma_chains_kernel<<<blocks, threads>>>(out, 16, 0.999999, 1e-7);  // warm-up
+        for (int rep = 0; rep < 3 && rc == PEARL_OK; ++rep) {
+            float ms = 0;
+            cudaEventRecord(e0);
+            fp64_fma_chains_kernel<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+            cudaEventRecord(e1);
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess ||
+                !(ms > 0))
+                rc = PEARL_ERR_CUDA;
+            else
+                best = std::max(best, 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12);
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(out);
+    if (rc == PEARL_OK && cudaGetLastError() != cudaSuccess) rc = PEARL_ERR_CUDA;
+    *tflops = best;
     return rc;
 }
 

@@ -399,21 +399,33 @@ __device__ __forceinline__ void init_pipe(const Pipe& pp) {
     mbar_fence_init();
 }
 
+// Bounded waits on a pipeline barrier.  A wait gives up after limit_ns, or
+// early once another warp of the block group has recorded a device-wait
+// timeout in *abort_status (a tile that warp left unfinished is never
+// refilled, so waiting out the full limit again would only double the time the
+// error path takes).  Drains of in-flight copies pass no abort_status: they
+// must wait for the copies themselves.
+__device__ __forceinline__ bool wait_aborted(const int* abort_status) {
+    return abort_status && *(const volatile int*)abort_status == (int)PEARL_ERR_DEVICE_WAIT;
+}
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  unsigned long long limit_ns = kBarrierTimeoutNs) {
+                                                  unsigned long long limit_ns = kBarrierTimeoutNs,
+                                                  const int* abort_status = nullptr) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned it = 1;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) return false;
+        if ((it & 63u) == 0 && (globaltimer_ns() - t0 > limit_ns || wait_aborted(abort_status))) return false;
     }
 }
-__device__ __forceinline__ bool mbar_wait_token_bounded(uint64_t* bar, uint64_t state) {
+__device__ __forceinline__ bool mbar_wait_token_bounded(uint64_t* bar, uint64_t state,
+                                                        const int* abort_status = nullptr) {
     if (mbar_try_wait_token(bar, state)) return true;
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned it = 1;; ++it) {
         if (mbar_try_wait_token(bar, state)) return true;
-        if ((it & 63u) == 0 && globaltimer_ns() - t0 > kBarrierTimeoutNs) return false;
+        if ((it & 63u) == 0 && (globaltimer_ns() - t0 > kBarrierTimeoutNs || wait_aborted(abort_status)))
+            return false;
     }
 }
 
@@ -475,11 +487,13 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
     for (int k = 0; k < nb; ++k) {
         const int s = k % S;
         if (!kWarpPipeline && threadIdx.x == 0 && k + S - 1 < nb) issue(k + S - 1);
-        if (!mbar_wait_bounded(&pp.bar[s], (pp.parity >> s) & 1u)) {
+        if (!mbar_wait_bounded(&pp.bar[s], (pp.parity >> s) & 1u, kBarrierTimeoutNs, &a.bar->status)) {
             atomicCAS(&a.bar->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
-            // drain the copies that may still be in flight (a tile is staged only
-            // once its stage's previous tile was finished by every warp), bounded
-            for (int j = k + 1; j < nb && j < k + S; ++j)
+            // drain the copies that may still be in flight, this tile's included
+            // when the wait was cut short by another warp's timeout (a tile is
+            // staged only once its stage's previous tile was finished by every
+            // warp), bounded
+            for (int j = k; j < nb && j < k + S; ++j)
                 mbar_wait_bounded(&pp.bar[j % S], (pp.parity >> (j % S)) & 1u, kBarrierTimeoutNs / 16);
             return false;
         }
@@ -519,7 +533,7 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
             const uint64_t token = mbar_arrive(&pp.empty[s]);
             const unsigned before = atomicAdd(&pp.cnt[s], 1u);
             if (before % kWarps == kWarps - 1 && k + S < nb) {
-                if (!mbar_wait_token_bounded(&pp.empty[s], token))
+                if (!mbar_wait_token_bounded(&pp.empty[s], token, &a.bar->status))
                     atomicCAS(&a.bar->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
                 else
                     issue(k + S);

@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "pearl_host.hpp"
 
 using namespace pearl_gpu;
@@ -36,6 +38,7 @@ constexpr int kNoAllocMaxDevices = 64;
 
 std::mutex g_noalloc_mutex;
 double* g_noalloc_device_ptr[kNoAllocMaxDevices] = {};
+CUcontext g_noalloc_device_ctx[kNoAllocMaxDevices] = {};
 
 }  // namespace
 
@@ -44,16 +47,38 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 namespace {
 
-// Device address of g_noalloc_scratch on the current device, looked up once per
-// device.  The host-side name is only a stand-in for the device symbol, so the
-// address must come from cudaGetSymbolAddress with that device current.
+// The CUDA context current on the calling thread (driver entry point, so the
+// library links no driver stub); null when it cannot be queried.
+CUcontext current_context() {
+    static PFN_cuCtxGetCurrent_v4000 get = nullptr;
+    if (!get) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return nullptr;
+        get = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    }
+    CUcontext c = nullptr;
+    return get(&c) == CUDA_SUCCESS ? c : nullptr;
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up on the
+// first call per device.  The host-side name is only a stand-in for the device
+// symbol, so the address must come from cudaGetSymbolAddress with that device
+// current.  The address belongs to the device's context: when that context
+// is replaced (cudaDeviceReset, or another library resetting the primary
+// context), the address is looked up again instead of reusing a dead one.
 int noalloc_scratch(int device, double** out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (device < 0 || device >= kNoAllocMaxDevices) return PEARL_ERR_NO_DEVICE;
-    if (!g_noalloc_device_ptr[device]) {
+    const CUcontext cur = current_context();
+    if (!g_noalloc_device_ptr[device] || cur != g_noalloc_device_ctx[device]) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PEARL_ERR_CUDA;
         g_noalloc_device_ptr[device] = static_cast<double*>(p);
+        // cudaGetSymbolAddress made the device's context current if none was
+        g_noalloc_device_ctx[device] = cur ? cur : current_context();
     }
     *out = g_noalloc_device_ptr[device];
     return PEARL_OK;

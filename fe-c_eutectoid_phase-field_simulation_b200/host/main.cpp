@@ -383,6 +383,10 @@ int main(int argc, char** argv) {
                "mu_max,cg_last,cg_peak,closure_last,rejected,shift_distance,wall_s\n";
         std::cout << "resources: ranks=1 layout=" << px << "x" << py << " grid=" << config.nx << "x" << config.ny
                   << "\n";
+        // Frames and checkpoints keep the reference's HDF5 object model but are
+        // not HDF5 files (libhdf5 is not linked): say so once, before the first.
+        std::cout << "NOTE: frame_*.h5 and checkpoint.h5 are written in the PEARL-H5-STUB container, not HDF5; "
+                     "HDF5 tools (h5py, ParaView) cannot open them\n";
         st.phi.resize(3 * cells);
         st.carbon.resize(cells);
         st.mu.resize(cells);

@@ -120,6 +120,7 @@ EXPORTS = [
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
     "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit", "pearl_gpu_batch_configure",
     "pearl_gpu_set_history", "pearl_gpu_get_history", "pearl_gpu_run_replay", "pearl_gpu_batch_plan",
+    "pearl_gpu_selftest_fp64_peak",
 ]
 
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -168,6 +169,7 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
     L.pearl_gpu_phase_times.argtypes = [V, DP, C.POINTER(C.c_longlong)]
     L.pearl_gpu_selftest_division.argtypes = [C.c_int, DP, DP, C.c_longlong, C.POINTER(C.c_ulonglong)]
+    L.pearl_gpu_selftest_fp64_peak.argtypes = [C.c_int, DP]
     L.pearl_gpu_smooth_interface.argtypes = [V, C.c_int, C.c_int, D, D, C.POINTER(PearlSmoothReport)]
     L.pearl_gpu_mixture_sums.argtypes = [V, DP, DP]
     L.pearl_gpu_init_composition.argtypes = [V, D, DP]
@@ -224,6 +226,15 @@ def selftest_division(a: np.ndarray, b: np.ndarray, device: int = 0) -> int:
     if rc:
         raise PearlError(rc, STATUS.get(rc, str(rc)))
     return int(n.value)
+
+
+def fp64_peak_tflops(device: int = 0) -> float:
+    """Measured FP64 throughput of the device (independent FMA chains, full grid)."""
+    t = C.c_double(0)
+    rc = library().pearl_gpu_selftest_fp64_peak(device, C.byref(t))
+    if rc:
+        raise PearlError(rc, STATUS.get(rc, str(rc)))
+    return t.value
 
 
 class PearlAdjointReport(C.Structure):

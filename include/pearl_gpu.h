@@ -242,6 +242,13 @@ int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* count
 int pearl_gpu_selftest_division(int device, const double* a, const double* b, long long n,
                                 unsigned long long* mismatches);
 
+/* FP64 throughput of `device`: independent FMA chains (8 per thread) in every
+ * thread of a full grid, timed with CUDA events; *tflops receives the best of
+ * three launches (an FMA counts two flops).  The roofline of the FP64-bound
+ * phases (propose_phi, the final update with its energy).  No reference
+ * counterpart. */
+int pearl_gpu_selftest_fp64_peak(int device, double* tflops);
+
 /* Self-test of the bounded device waits, on this context's grid and control
  * block: launches a grid barrier that waits for one block more than the grid
  * has, so every block must give up after the barrier's time limit (4 s).
@@ -267,7 +274,9 @@ int pearl_gpu_selftest_wait_limit(pearl_gpu_ctx* ctx, int* status, double* waite
  * held by every GPU that loads the library until the process exits), so
  * nx*ny is limited to 262144 cells; larger domains return PEARL_ERR_TOO_LARGE.
  * The first call on each device looks up that array's device address; make
- * that first call before any stream capture.  All calls on a device share the
+ * that first call before any stream capture.  The address is looked up again
+ * when the device's CUDA context has changed since (after cudaDeviceReset),
+ * so that call too must come before any capture.  All calls on a device share the
  * same scratch, so calls that overlap on the GPU (other streams or threads)
  * race and must be serialised by the caller. */
 int pearl_gpu_advance_noalloc(const pearl_params* params, int nx, int ny, double* d_phi, double* d_carbon,

@@ -1,10 +1,9 @@
 """Per-field error of the mixed-precision form against the FP64 GPU path and,
-optionally, the FP64 CPU oracle, after N steps of the same workload.
+optionally, the FP64 CPU oracle, after N steps of the same workload (a test
+helper: it runs the oracle, so it lives with the tests, not in the package).
 
-    python fe-c_eutectoid_phase-field_simulation_b200/pearl_gpu/precision_report.py \
-        --nx 128 --ny 256 --small --steps 20000 --oracle
-    python fe-c_eutectoid_phase-field_simulation_b200/pearl_gpu/precision_report.py \
-        --nx 4096 --ny 8192 --pairs 128 --steps 20000
+    python tests/precision_report.py --small --steps 20000 --oracle
+    python tests/precision_report.py --nx 4096 --ny 8192 --pairs 128 --steps 20000
 
 --small uses the 128x256 fixed-dt workload (10 K, 4 pairs); otherwise the large
 adaptive workload (20 K, seeded spacing and front jitter) at the given size.
@@ -22,9 +21,10 @@ from pathlib import Path
 
 import numpy as np
 
-sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
-ROOT = Path(__file__).resolve().parent.parent.parent
-sys.path.insert(0, str(ROOT))
+ROOT = Path(__file__).resolve().parent.parent
+for _p in (str(ROOT), str(ROOT / "fe-c_eutectoid_phase-field_simulation_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
 
 
 def _err(a, b):

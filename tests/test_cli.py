@@ -160,6 +160,8 @@ def test_cli_smoke_run_matches_reference(cli, tmp_path):
     ref = json.loads((GOLDEN / "smoke_golden.json").read_text())
     p, out = _run(cli, cli_inputs.case_smoke(), [], tmp_path, "smoke")
     assert p.returncode == 0, p.stderr
+    # the frames are not HDF5: the run says so once
+    assert p.stdout.count("written in the PEARL-H5-STUB container, not HDF5") == 1
     assert sorted(x.name for x in out.iterdir()) == ref["files"]
     assert (out / "COMPLETED.txt").read_text() == ref["completed"]
     head, rows = _csv((out / "diagnostics.csv").read_text())

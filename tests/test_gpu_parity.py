@@ -117,6 +117,38 @@ def test_advance_small_fixed_dt(gpu_lib, port):
     assert sum(i.retries for i in infos) >= 1
 
 
+def test_small_workload_full_horizon(gpu_lib, port):
+    """The small FP64 configuration at its own horizon: 128x256, 4 pairs, 10 K,
+    fixed dt = dt_max = 4e-12 s, 2000 accepted steps in persistent launches of
+    500 steps, against the oracle's 2000 steps (about 20 s of CPU): every step's
+    retries, dt and CG count agree, and the fields meet the FP64 bars."""
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    w = workloads.plain_small()
+    n = w.meta["steps"]
+    assert n == 2000
+    with _ctx(w) as ctx:
+        ctx.set_history(n)
+        done = 0
+        while done < n:
+            done += ctx.run(min(500, n - done)).steps
+        infos, recorded = ctx.history()
+        phi, c, mu, s = ctx.download()
+    assert recorded == n
+    po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    so = pyoracle.scalars_from(w.scalars)
+    rc, why, done, oinfos = port.advance_n(w.params, po, co, muo, so, n)
+    assert rc == 0 and done == n, why
+    assert [i.retries for i in infos] == [i.retries for i in oinfos]
+    assert [i.accepted_dt for i in infos] == [i.accepted_dt for i in oinfos]
+    assert [i.cg_iterations for i in infos] == [i.cg_iterations for i in oinfos]
+    assert s.step == so.step and s.rejected == so.rejected and s.time == so.time
+    assert np.abs(phi - po).max() <= PHI_TOL
+    assert np.abs(mu - muo).max() <= MU_TOL
+    assert abs(c.sum() - co.sum()) <= MASS_RTOL * abs(co.sum())
+
+
 def _adaptive():
     from pearl_gpu import workloads
 
@@ -179,16 +211,20 @@ def test_smallest_and_ragged_domains(gpu_lib, port, nx, ny, front):
 
 def test_full_size_large_workload_replay(gpu_lib, port):
     """The large FP64 configuration at its full size (2048x4096, 64 pairs,
-    20 K, adaptive dt): 4 accepted steps on the GPU through the run loop, then
-    the oracle replays the GPU's accepted dt sequence on the host and the
-    fields are held to the FP64 bars (about 15 s of CPU)."""
+    20 K, adaptive dt): 30 accepted steps on the GPU in one persistent launch,
+    then the oracle replays the GPU's accepted dt sequence on the host (about
+    90 s of CPU) with the same CG counts, and the fields are held to the FP64
+    bars."""
     from oracle import pyoracle
     from pearl_gpu import workloads
 
     w = workloads.plain_large()
-    n = 4
+    n = 30
     with _ctx(w) as ctx:
-        infos = [ctx.advance() for _ in range(n)]
+        ctx.set_history(n)
+        assert ctx.run(n).steps == n
+        infos, recorded = ctx.history()
+        assert recorded == n
         phi, c, mu, s = ctx.download()
     po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
     so = pyoracle.scalars_from(w.scalars)

@@ -5,7 +5,13 @@ planes; the library's scratch is a fixed array compiled into it.
 
 Checked here through the C ABI against the context-based entry point
 (pearl_gpu_advance) on the same input, for two calls in a row, with the
-tolerances of the other parity tests.  This file is collected last.
+tolerances of the other parity tests.  The context pads every row to a
+multiple of 32 doubles; this entry point runs on the caller's dense rows
+(pitch = nx), so widths that are not multiples of 32 (37, 100, 513) exercise
+its own row layout and periodic x wrap.  A phase-only case covers the trial
+carbon and mu that the proposal itself writes into the scratch.  After the
+first call, a second call must leave the device's free memory unchanged.
+This file is collected last.
 """
 from __future__ import annotations
 
@@ -43,22 +49,41 @@ def _noalloc_step(lib, params, w, phi, c, mu, scalars):
     return rc, info
 
 
-def test_noalloc_matches_context_entry_point(gpu_lib):
+CASES = [
+    # (nx, ny, front, extra controls)
+    (96, 72, 20.0, {}),
+    (100, 72, 20.0, {}),         # row length not a multiple of 32
+    (37, 19, 6.0, {}),           # ragged in both directions, smaller than one tile
+    (513, 511, 40.0, {}),        # 262143 cells: just under the scratch limit
+    (100, 72, 20.0, {"phase_only": 1}),
+]
+
+
+@pytest.mark.parametrize("nx,ny,front,controls", CASES,
+                         ids=["96x72", "100x72", "37x19", "513x511", "100x72-phase-only"])
+def test_noalloc_matches_context_entry_point(gpu_lib, nx, ny, front, controls):
     import torch
 
     import pearl_gpu
     from pearl_gpu import workloads
 
     torch.cuda.set_device(0)
-    w = workloads.scaled(96, 72, seed=4, front=20.0, jitter=0.1, front_jitter=1)
+    w = workloads.scaled(nx, ny, seed=4, front=front, jitter=0.1, front_jitter=1, **controls)
     params = pearl_gpu.PearlParams.from_dict(w.params)
     phi, c, mu = _planes(w)
     scalars = pearl_gpu.PearlScalars.from_dict(w.scalars)
     with pearl_gpu.Context(w.params, w.nx, w.ny, device=0) as ctx:
         ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
-        for _ in range(2):
+        for call in range(2):
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             rc, info = _noalloc_step(gpu_lib, params, w, phi, c, mu, scalars)
             assert rc == 0, pearl_gpu.STATUS.get(rc, rc)
+            free_after = torch.cuda.mem_get_info()[0]
+            if call == 1:
+                # the first call may load the library's module (and its static
+                # scratch) onto the device; later calls allocate nothing
+                assert free_after == free_before
             ref = ctx.advance()
             assert info.retries == ref.retries
             assert info.cg_iterations == ref.cg_iterations
