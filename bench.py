@@ -743,7 +743,9 @@ def probe_arm(args) -> None:
                 ctx.propose_phi(dt)
                 d = ctx.implicit_diffusion(dt)
                 out = {"probe": "diffusion", "ok": d["ok"], "cg_iterations": d["it"]}
-            out.update(nx=w.nx, ny=w.ny, precision=args.precision, kernel_ms=ctx.stats()["last_ms"])
+            out.update(nx=w.nx, ny=w.ny, precision=args.precision, kernel_ms=ctx.stats()["last_ms"],
+                       geometry=ctx.geometry(),
+                       phase_ms={k: round(v[0], 4) for k, v in ctx.phase_times().items()})
             print(json.dumps(out), flush=True)
 
 

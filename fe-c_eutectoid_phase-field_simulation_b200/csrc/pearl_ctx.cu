@@ -374,6 +374,154 @@ int download_set(pearl_gpu_ctx* ctx, int set, double* phi, double* carbon, doubl
 
 }  // namespace pearl_gpu
 
+// ------------------------------------------------------------------ filling commands
+// One filling command on the device: its parameters plus the cosine and sine
+// of its angles, taken on the host with the reference's expressions
+// (angle*pi/180, std::cos, std::sin), so every cell sees the same directions
+// as the reference.
+struct DevFillOp {
+    int method;
+    double p[PEARL_FILL_MAX_PARAMS];
+    double ux[3], uy[3];
+};
+
+// filling_centered_lamellar_phase (pearl_serial.cpp:1378-1388)
+__device__ __forceinline__ int fill_centered_lamellar(double along, double period, double fraction, int ferrite,
+                                                      int cementite) {
+    double pos = fmod(along, period);
+    if (pos < 0.0) pos += period;
+    const double width = fraction * period;
+    const double start = 0.5 * (period - width), end = 0.5 * (period + width);
+    return pos >= start && pos < end ? cementite : ferrite;
+}
+
+// filling_phase_at (pearl_serial.cpp:1393-1514) of cell (gx, gy): the label of
+// the last command that paints the cell, gamma (2) where none does.  Every
+// comparison and product follows the reference's expressions and order.
+__device__ int fill_label(const DevFillOp* ops, int nops, int gx, int gy) {
+    const double pi = 3.14159265358979323846;
+    int label = 2;
+    for (int k = 0; k < nops; ++k) {
+        const DevFillOp& o = ops[k];
+        const double* p = o.p;
+        if (o.method == PEARL_FILL_CUBE) {
+            const int sel = (int)p[0];
+            if (sel != 2 && gx >= p[1] && gx <= p[4] && gy >= p[2] && gy <= p[5]) label = sel;
+        } else if (o.method == PEARL_FILL_CYLINDER) {
+            const double dx = gx - p[1], dy = gy - p[2];
+            const int sel = (int)p[0];
+            if (sel != 2 && dx * dx + dy * dy <= p[5] * p[5]) label = sel;
+        } else if (o.method == PEARL_FILL_CENTER_BOX_2D) {
+            const bool inside = gx >= p[0] && gx < p[1] && gy >= p[2] && gy < p[3];
+            label = (int)(inside ? p[4] : p[5]);
+        } else if (o.method == PEARL_FILL_Y_JUNCTION_2D || o.method == PEARL_FILL_Y_JUNCTION_LAMELLAE_2D) {
+            const bool lam = o.method == PEARL_FILL_Y_JUNCTION_LAMELLAE_2D;
+            const int ferrite = (int)p[lam ? 13 : 11];
+            label = (int)p[lam ? 15 : 12];
+            if (!(gx >= p[0] && gx < p[1] && gy >= p[2] && gy < p[3])) continue;
+            const double dx = gx - p[4], dy = gy - p[5];
+            for (int arm = 0; arm < 3; ++arm) {
+                const double along = dx * o.ux[arm] + dy * o.uy[arm];
+                const double across = -dx * o.uy[arm] + dy * o.ux[arm];
+                if (along >= 0.0 && along <= p[9] && fabs(across) <= p[10]) {
+                    int sel = ferrite;
+                    if (lam) {
+                        const double period = p[11] + p[12];
+                        double pos = fmod(along, period);
+                        if (pos < 0.0) pos += period;
+                        if (!(pos < p[11])) sel = (int)p[14];
+                    }
+                    label = sel;
+                    break;  // the first arm that contains the cell wins
+                }
+            }
+        } else if (o.method == PEARL_FILL_ADHERED_PEARLITE_ARM_2D) {
+            const double dx = gx - p[0], dy = gy - p[1];
+            const double along = dx * o.ux[0] + dy * o.uy[0];
+            const double across = -dx * o.uy[0] + dy * o.ux[0];
+            const double arm_length = p[3];
+            const int pairs = (int)p[4];
+            const double period = arm_length / (double)pairs;
+            const double ferrite_width = (1.0 - p[5]) * period, cementite_width = p[5] * period;
+            const double peak = p[6], contact = p[7], bridge = p[8];
+            const int ferrite = (int)p[9], cementite = (int)p[10];
+            int sel = -1;
+            if (along >= 0.0 && along <= arm_length) {
+                int pair = along >= arm_length ? pairs - 1 : (int)floor(along / period);
+                pair = max(0, min(pairs - 1, pair));
+                const double pair_start = (double)pair * period;
+                const double local = along - pair_start;
+                int segment;
+                double seg_start, seg_len;
+                if (local < ferrite_width) {
+                    segment = 2 * pair;
+                    seg_start = pair_start;
+                    seg_len = ferrite_width;
+                    sel = ferrite;
+                } else {
+                    segment = 2 * pair + 1;
+                    seg_start = pair_start + ferrite_width;
+                    seg_len = cementite_width;
+                    sel = cementite;
+                }
+                double frac = (along - seg_start) / seg_len;
+                if (frac < 0.0)
+                    frac = 0.0;
+                else if (frac > 1.0)
+                    frac = 1.0;
+                const double h0 = segment == 0 ? 0.0 : contact;
+                const double h1 = segment == 2 * pairs - 1 ? 0.0 : contact;
+                const double mean_end = 0.5 * (h0 + h1);
+                double half = (1.0 - frac) * h0 + frac * h1 + (peak - mean_end) * sin(pi * frac);
+                if (half > peak) half = peak;
+                if (fabs(across) > half) sel = -1;
+            }
+            if (bridge > 0.0) {
+                const double r2 = bridge * bridge;
+                const double d_start = along * along + across * across;
+                const double d_end = (along - arm_length) * (along - arm_length) + across * across;
+                if (d_start <= r2) sel = ferrite;
+                if (d_end <= r2) sel = cementite;
+            }
+            if (sel >= 0) label = sel;
+        } else if (o.method == PEARL_FILL_PEARLITE_ELLIPSE_2D) {
+            const double dx = gx - p[0], dy = gy - p[1];
+            const double along = dx * o.ux[0] + dy * o.uy[0];
+            const double across = -dx * o.uy[0] + dy * o.ux[0];
+            const double start = p[3], period = p[5], length = p[4] * period;
+            const double semi_major = 0.5 * length, semi_minor = p[6] * semi_major;
+            const double centre = start + semi_major;
+            const double na = (along - centre) / semi_major;
+            const double nc = across / semi_minor;
+            const double bridge = p[8];
+            const int ferrite = (int)p[9], cementite = (int)p[10];
+            int sel = -1;
+            if (na * na + nc * nc <= 1.0) sel = fill_centered_lamellar(along - start, period, p[7], ferrite, cementite);
+            if (bridge > 0.0) {
+                const double ds = (along - start) * (along - start) + across * across;
+                const double de = (along - (start + length)) * (along - (start + length)) + across * across;
+                if (ds <= bridge * bridge || de <= bridge * bridge) sel = ferrite;
+            }
+            if (sel >= 0) label = sel;
+        }
+    }
+    return label;
+}
+
+// One-hot phase fractions of every cell's label into the padded planes.
+__global__ void fill_kernel(const DevFillOp* ops, int nops, int nx, int ny, int pitch, double* pa, double* pt,
+                            double* pg) {
+    const long long n = (long long)nx * ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)(i / nx);
+        const int label = fill_label(ops, nops, x, y);
+        const size_t j = (size_t)y * pitch + x;
+        pa[j] = label == 0 ? 1.0 : 0.0;
+        pt[j] = label == 1 ? 1.0 : 0.0;
+        pg[j] = label == 2 ? 1.0 : 0.0;
+    }
+}
+
 // FP64 throughput probe: eight independent FMA chains per thread, so the FP64
 // pipe, not the dependency latency, bounds the loop.
 __global__ void fp64_fma_chains_kernel(double* out, int iters, double a, double b) {
@@ -505,6 +653,7 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->d_fill) cudaFree(ctx->d_fill);
     if (ctx->d_hist) cudaFree(ctx->d_hist);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -750,6 +899,53 @@ int pearl_gpu_mixture_sums(pearl_gpu_ctx* ctx, double* sum_c_intercept, double* 
     return PEARL_OK;
 }
 
+int pearl_gpu_fill(pearl_gpu_ctx* ctx, const pearl_fill_op* ops, int nops) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    if (nops < 0 || nops > PEARL_FILL_MAX_OPS || (nops > 0 && !ops))
+        return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid filling command list");
+    // parameter counts of validate_filling_operations (pearl_serial.cpp:1299-1343)
+    static const int kCount[8] = {0, 7, 6, 6, 13, 16, 11, 11};
+    const double pi = 3.14159265358979323846;
+    std::vector<DevFillOp> h((size_t)std::max(nops, 1));
+    for (int k = 0; k < nops; ++k) {
+        const pearl_fill_op& o = ops[k];
+        if (o.method < PEARL_FILL_CUBE || o.method > PEARL_FILL_PEARLITE_ELLIPSE_2D || o.nparams != kCount[o.method])
+            return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "unsupported filling method or parameter count");
+        DevFillOp& d = h[(size_t)k];
+        std::memset(&d, 0, sizeof d);
+        d.method = o.method;
+        for (int j = 0; j < o.nparams; ++j) d.p[j] = o.p[j];
+        // the arms' directions, as filling_phase_at forms them (:1421-1422, :1441-1442, :1491-1492)
+        if (o.method == PEARL_FILL_Y_JUNCTION_2D || o.method == PEARL_FILL_Y_JUNCTION_LAMELLAE_2D) {
+            for (int arm = 0; arm < 3; ++arm) {
+                const double ang = o.p[6 + arm] * pi / 180.0;
+                d.ux[arm] = std::cos(ang);
+                d.uy[arm] = std::sin(ang);
+            }
+        } else if (o.method == PEARL_FILL_ADHERED_PEARLITE_ARM_2D || o.method == PEARL_FILL_PEARLITE_ELLIPSE_2D) {
+            const double ang = o.p[2] * pi / 180.0;
+            d.ux[0] = std::cos(ang);
+            d.uy[0] = std::sin(ang);
+        }
+    }
+    PG_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (!ctx->d_fill) PG_CUDA(ctx, cudaMalloc(&ctx->d_fill, sizeof(DevFillOp) * PEARL_FILL_MAX_OPS));
+    if (nops > 0)
+        PG_CUDA(ctx, cudaMemcpyAsync(ctx->d_fill, h.data(), sizeof(DevFillOp) * nops, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    const int cur = ctx->h_ctl->cur;
+    fill_kernel<<<stage_grid(ctx), 256, 0, ctx->stream>>>(static_cast<const DevFillOp*>(ctx->d_fill), nops, ctx->nx,
+                                                          ctx->ny, ctx->pitch, ctx->B.phi[cur][0], ctx->B.phi[cur][1],
+                                                          ctx->B.phi[cur][2]);
+    ctx->launches++;
+    PG_CUDA(ctx, cudaGetLastError());
+    ctx->h_ctl->energy_valid = 0;
+    int rc = push_ctl(ctx);
+    if (rc) return rc;
+    PG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PEARL_OK;
+}
+
 int pearl_gpu_init_composition(pearl_gpu_ctx* ctx, double mu, double* total_carbon) {
     if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
     KArgs a{};
@@ -931,6 +1127,14 @@ int pearl_gpu_phase_times(const pearl_gpu_ctx* ctx, double* ms, long long* count
         if (ms) ms[k] = k < kTagCount ? ctx->h_ctl->phase_ns[k] * 1e-6 : 0.0;
         if (counts) counts[k] = k < kTagCount ? (long long)ctx->h_ctl->phase_count[k] : 0;
     }
+    return PEARL_OK;
+}
+
+int pearl_gpu_geometry(const pearl_gpu_ctx* ctx, int* warps, int* warps_x_log2, int* grid_blocks) {
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    if (warps) *warps = ctx->warps;
+    if (warps_x_log2) *warps_x_log2 = ctx->P.warps_x_log2;
+    if (grid_blocks) *grid_blocks = ctx->grid;
     return PEARL_OK;
 }
 

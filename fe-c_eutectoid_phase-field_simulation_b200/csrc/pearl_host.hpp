@@ -40,6 +40,7 @@ struct pearl_gpu_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int adj_grid = 0;  // cooperative grid of the adjoint kernel (0 until first use)
     pearl_step_info* d_hist = nullptr;  // per-step history ring (pearl_gpu_set_history)
+    void* d_fill = nullptr;             // filling commands of pearl_gpu_fill (PEARL_FILL_MAX_OPS)
     long long hist_cap = 0, hist_count = 0;
     std::string error;
 };

@@ -288,141 +288,6 @@ void validate_fill(const std::vector<FillOp>& ops, int nx, int ny) {
     }
 }
 
-namespace {
-std::array<double, 3> one_hot(int phase) {
-    std::array<double, 3> f{0.0, 0.0, 0.0};
-    f[phase] = 1.0;
-    return f;
-}
-int centered_lamellar_phase(double along, double period, double cementite_fraction, int ferrite, int cementite) {
-    double pos = std::fmod(along, period);
-    if (pos < 0.0) pos += period;
-    const double width = cementite_fraction * period;
-    const double start = 0.5 * (period - width), end = 0.5 * (period + width);
-    return pos >= start && pos < end ? cementite : ferrite;
-}
-}  // namespace
-
-std::array<double, 3> fill_phase_at(const std::vector<FillOp>& ops, int gx, int gy) {
-    std::array<double, 3> f = one_hot(2);
-    const double pi = 3.14159265358979323846;
-    for (const auto& op : ops) {
-        const auto& p = op.p;
-        const std::string& m = op.method;
-        if (m == "FILLCUBE") {
-            const int sel = static_cast<int>(p[0]);
-            if (sel != 2 && gx >= p[1] && gx <= p[4] && gy >= p[2] && gy <= p[5]) f = one_hot(sel);
-        } else if (m == "FILLCYLINDER") {
-            const double dx = gx - p[1], dy = gy - p[2];
-            const int sel = static_cast<int>(p[0]);
-            if (sel != 2 && dx * dx + dy * dy <= p[5] * p[5]) f = one_hot(sel);
-        } else if (m == "FILLCENTERBOX2D") {
-            const bool inside = gx >= p[0] && gx < p[1] && gy >= p[2] && gy < p[3];
-            f = one_hot(static_cast<int>(inside ? p[4] : p[5]));
-        } else if (m == "FILLYJUNCTION2D" || m == "FILLYJUNCTIONLAMELLAE2D") {
-            const bool lam = m == "FILLYJUNCTIONLAMELLAE2D";
-            const int ferrite = static_cast<int>(p[lam ? 13 : 11]);
-            const int austenite = static_cast<int>(p[lam ? 15 : 12]);
-            f = one_hot(austenite);
-            if (!(gx >= p[0] && gx < p[1] && gy >= p[2] && gy < p[3])) continue;
-            const double dx = gx - p[4], dy = gy - p[5];
-            for (int arm = 0; arm < 3; ++arm) {
-                const double ang = p[6 + arm] * pi / 180.0;
-                const double ux = std::cos(ang), uy = std::sin(ang);
-                const double along = dx * ux + dy * uy;
-                const double across = -dx * uy + dy * ux;
-                if (along >= 0.0 && along <= p[9] && std::fabs(across) <= p[10]) {
-                    int sel = ferrite;
-                    if (lam) {
-                        const double period = p[11] + p[12];
-                        double pos = std::fmod(along, period);
-                        if (pos < 0.0) pos += period;
-                        if (!(pos < p[11])) sel = static_cast<int>(p[14]);
-                    }
-                    f = one_hot(sel);
-                    break;  // the first arm that contains the cell wins
-                }
-            }
-        } else if (m == "FILLADHEREDPEARLITEARM2D") {
-            const double ang = p[2] * pi / 180.0;
-            const double ux = std::cos(ang), uy = std::sin(ang);
-            const double dx = gx - p[0], dy = gy - p[1];
-            const double along = dx * ux + dy * uy;
-            const double across = -dx * uy + dy * ux;
-            const double arm_length = p[3];
-            const int pairs = static_cast<int>(p[4]);
-            const double period = arm_length / static_cast<double>(pairs);
-            const double ferrite_width = (1.0 - p[5]) * period, cementite_width = p[5] * period;
-            const double peak = p[6], contact = p[7], bridge = p[8];
-            const int ferrite = static_cast<int>(p[9]), cementite = static_cast<int>(p[10]);
-            int sel = -1;
-            if (along >= 0.0 && along <= arm_length) {
-                int pair = along >= arm_length ? pairs - 1 : static_cast<int>(std::floor(along / period));
-                pair = std::max(0, std::min(pairs - 1, pair));
-                const double pair_start = static_cast<double>(pair) * period;
-                const double local = along - pair_start;
-                int segment;
-                double seg_start, seg_len;
-                if (local < ferrite_width) {
-                    segment = 2 * pair;
-                    seg_start = pair_start;
-                    seg_len = ferrite_width;
-                    sel = ferrite;
-                } else {
-                    segment = 2 * pair + 1;
-                    seg_start = pair_start + ferrite_width;
-                    seg_len = cementite_width;
-                    sel = cementite;
-                }
-                double frac = (along - seg_start) / seg_len;
-                if (frac < 0.0)
-                    frac = 0.0;
-                else if (frac > 1.0)
-                    frac = 1.0;
-                const double h0 = segment == 0 ? 0.0 : contact;
-                const double h1 = segment == 2 * pairs - 1 ? 0.0 : contact;
-                const double mean_end = 0.5 * (h0 + h1);
-                double half = (1.0 - frac) * h0 + frac * h1 + (peak - mean_end) * std::sin(pi * frac);
-                if (half > peak) half = peak;
-                if (std::fabs(across) > half) sel = -1;
-            }
-            if (bridge > 0.0) {
-                const double r2 = bridge * bridge;
-                const double d_start = along * along + across * across;
-                const double d_end = (along - arm_length) * (along - arm_length) + across * across;
-                if (d_start <= r2) sel = ferrite;
-                if (d_end <= r2) sel = cementite;
-            }
-            if (sel >= 0) f = one_hot(sel);
-        } else if (m == "FILLPEARLITEELLIPSE2D") {
-            const double ang = p[2] * pi / 180.0;
-            const double ux = std::cos(ang), uy = std::sin(ang);
-            const double dx = gx - p[0], dy = gy - p[1];
-            const double along = dx * ux + dy * uy;
-            const double across = -dx * uy + dy * ux;
-            const double start = p[3], period = p[5], length = p[4] * period;
-            const double semi_major = 0.5 * length, semi_minor = p[6] * semi_major;
-            const double centre = start + semi_major;
-            const double na = (along - centre) / semi_major;
-            const double nc = across / semi_minor;
-            const double bridge = p[8];
-            const int ferrite = static_cast<int>(p[9]), cementite = static_cast<int>(p[10]);
-            int sel = -1;
-            if (na * na + nc * nc <= 1.0)
-                sel = centered_lamellar_phase(along - start, period, p[7], ferrite, cementite);
-            if (bridge > 0.0) {
-                const double ds = (along - start) * (along - start) + across * across;
-                const double de = (along - (start + length)) * (along - (start + length)) + across * across;
-                if (ds <= bridge * bridge || de <= bridge * bridge) sel = ferrite;
-            }
-            if (sel >= 0) f = one_hot(sel);
-        } else {
-            throw std::invalid_argument("Unvalidated/unsupported filling method: " + m);
-        }
-    }
-    return f;
-}
-
 // ------------------------------------------------------------------ signature
 std::string Config::physics_signature() const {
     std::ostringstream o;

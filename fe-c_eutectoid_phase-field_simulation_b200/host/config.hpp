@@ -74,10 +74,10 @@ Parabola at_undercooling(const Parabola& reference, const GrandPotential& slope,
 Thermo at_phase_diagram_undercooling(const Thermo& reference, const PhaseDiagram& diagram, double undercooling);
 GrandPotential to_grand_potential(const Parabola& p);
 
-// FILL geometry (pearl_serial.cpp:1181-1515).
+// FILL commands (pearl_serial.cpp:1181-1349); the cells are painted on the
+// device (pearl_gpu_fill, filling_phase_at :1393-1514).
 FillOp parse_fill(const std::string& method, const std::string& value, int line);
 void validate_fill(const std::vector<FillOp>& ops, int nx, int ny);
-std::array<double, 3> fill_phase_at(const std::vector<FillOp>& ops, int x, int y);
 
 // Obstacle profile used by the native initialisations (pearl_serial.cpp:563-569).
 double profile(double distance, double epsilon);

@@ -147,6 +147,32 @@ std::array<double, 3> phase_fractions(const Config& c, const std::vector<double>
     return out;
 }
 
+// The input's filling commands in the C ABI's form (method code + parameters).
+std::vector<pearl_fill_op> device_fill_ops(const std::vector<FillOp>& fill) {
+    static const std::pair<const char*, int> kMethods[] = {
+        {"FILLCUBE", PEARL_FILL_CUBE},
+        {"FILLCYLINDER", PEARL_FILL_CYLINDER},
+        {"FILLCENTERBOX2D", PEARL_FILL_CENTER_BOX_2D},
+        {"FILLYJUNCTION2D", PEARL_FILL_Y_JUNCTION_2D},
+        {"FILLYJUNCTIONLAMELLAE2D", PEARL_FILL_Y_JUNCTION_LAMELLAE_2D},
+        {"FILLADHEREDPEARLITEARM2D", PEARL_FILL_ADHERED_PEARLITE_ARM_2D},
+        {"FILLPEARLITEELLIPSE2D", PEARL_FILL_PEARLITE_ELLIPSE_2D},
+    };
+    if (fill.size() > PEARL_FILL_MAX_OPS) throw std::invalid_argument("too many filling commands");
+    std::vector<pearl_fill_op> ops;
+    for (const auto& f : fill) {
+        pearl_fill_op o{};
+        for (const auto& m : kMethods)
+            if (f.method == m.first) o.method = m.second;
+        if (!o.method || f.p.size() > PEARL_FILL_MAX_PARAMS)
+            throw std::invalid_argument("Unvalidated/unsupported filling method: " + f.method);
+        o.nparams = static_cast<int>(f.p.size());
+        for (size_t j = 0; j < f.p.size(); ++j) o.p[j] = f.p[j];
+        ops.push_back(o);
+    }
+    return ops;
+}
+
 // Native initial geometry (pearl_serial.cpp:1764-1794).
 std::vector<double> initial_geometry(const Config& c) {
     std::vector<double> phi(static_cast<size_t>(c.nx) * c.ny * 3, 0.0);
@@ -160,7 +186,7 @@ std::vector<double> initial_geometry(const Config& c) {
                 const double th = profile(dist, eps), product = profile(yy - c.seed_height, eps);
                 p = {(1 - th) * product, th * product, 1 - product};
             } else if (c.initialization == "microsim") {
-                p = fill_phase_at(c.fill, x, y);
+                p = {0, 0, 1};  // painted on the device by pearl_gpu_fill
             } else if (c.initialization == "sharp_smooth") {
                 const bool product = yy < c.seed_height;
                 if (!product)
@@ -257,6 +283,12 @@ int main(int argc, char** argv) {
             st.carbon.assign(cells, 0.0);
             st.mu.assign(cells, 0.0);
             gpu.check(pearl_gpu_upload(gpu.ctx, st.phi.data(), st.carbon.data(), st.mu.data(), nullptr));
+            if (config.initialization == "microsim") {
+                // filling_phase_at of every cell (pearl_serial.cpp:1771-1772) on the device
+                const std::vector<pearl_fill_op> ops = device_fill_ops(config.fill);
+                gpu.check(pearl_gpu_fill(gpu.ctx, ops.data(), static_cast<int>(ops.size())));
+                gpu.check(pearl_gpu_download(gpu.ctx, st.phi.data(), nullptr, nullptr, nullptr));
+            }
             if (config.initialization == "sharp_smooth" || config.initialization == "microsim") {
                 write_initial_phases(config.nx, config.ny, config.dx, config.dy, st.phi,
                                      fs::path(output) / "init_sharp.h5", "init_sharp", 0);

@@ -120,8 +120,25 @@ EXPORTS = [
     "pearl_gpu_batch_stats", "pearl_gpu_batch_last_error", "pearl_gpu_adjoint_gradient", "pearl_gpu_set_precision",
     "pearl_gpu_batch_set_precision", "pearl_gpu_selftest_wait_limit", "pearl_gpu_batch_configure",
     "pearl_gpu_set_history", "pearl_gpu_get_history", "pearl_gpu_run_replay", "pearl_gpu_batch_plan",
-    "pearl_gpu_selftest_fp64_peak",
+    "pearl_gpu_selftest_fp64_peak", "pearl_gpu_geometry", "pearl_gpu_fill",
 ]
+
+# Filling commands (PEARL_FILL_*): method name -> code
+FILL_METHODS = {"FILLCUBE": 1, "FILLCYLINDER": 2, "FILLCENTERBOX2D": 3, "FILLYJUNCTION2D": 4,
+                "FILLYJUNCTIONLAMELLAE2D": 5, "FILLADHEREDPEARLITEARM2D": 6, "FILLPEARLITEELLIPSE2D": 7}
+
+
+class PearlFillOp(C.Structure):
+    _fields_ = [("method", C.c_int), ("nparams", C.c_int), ("p", D * 16)]
+
+    @classmethod
+    def make(cls, method: str, params) -> "PearlFillOp":
+        o = cls()
+        o.method = FILL_METHODS[method]
+        o.nparams = len(params)
+        for j, v in enumerate(params):
+            o.p[j] = float(v)
+        return o
 
 PRECISION = {"fp64": 0, "mixed": 1}
 # Batch group_blocks value for groups sized per instance (PEARL_BATCH_SIZED_GROUPS)
@@ -167,6 +184,8 @@ def library(path: Path | None = None) -> C.CDLL:
     L.pearl_gpu_last_error.argtypes = [V]
     L.pearl_gpu_last_error.restype = C.c_char_p
     L.pearl_gpu_stats.argtypes = [V, C.POINTER(C.c_longlong), C.POINTER(C.c_int), DP]
+    L.pearl_gpu_geometry.argtypes = [V, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.pearl_gpu_fill.argtypes = [V, C.POINTER(PearlFillOp), C.c_int]
     L.pearl_gpu_phase_times.argtypes = [V, DP, C.POINTER(C.c_longlong)]
     L.pearl_gpu_selftest_division.argtypes = [C.c_int, DP, DP, C.c_longlong, C.POINTER(C.c_ulonglong)]
     L.pearl_gpu_selftest_fp64_peak.argtypes = [C.c_int, DP]
@@ -354,6 +373,12 @@ class Context:
                                                         C.byref(rep)))
         return rep
 
+    def fill(self, commands) -> None:
+        """Paint the current phase fields with filling commands [(method, params), ...]
+        (pearl_gpu_fill: filling_phase_at of every cell, on the device)."""
+        ops = (PearlFillOp * max(len(commands), 1))(*[PearlFillOp.make(m, p) for m, p in commands])
+        self._check(self.lib.pearl_gpu_fill(self.h, ops, len(commands)))
+
     def mixture_sums(self):
         a, b = D(), D()
         self._check(self.lib.pearl_gpu_mixture_sums(self.h, C.byref(a), C.byref(b)))
@@ -441,6 +466,13 @@ class Context:
         cnt = (C.c_longlong * 16)()
         self._check(self.lib.pearl_gpu_phase_times(self.h, ms, cnt))
         return {name: (ms[k], cnt[k]) for k, name in enumerate(PHASES) if cnt[k]}
+
+    def geometry(self) -> dict:
+        """warps per block, warps side by side in x (log2) and grid blocks: the
+        tree every global sum follows (oracle: set_device_order)."""
+        w, wx, g = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.pearl_gpu_geometry(self.h, C.byref(w), C.byref(wx), C.byref(g)))
+        return dict(warps=w.value, warps_x_log2=wx.value, blocks=g.value)
 
     def stats(self):
         n, g, ms = C.c_longlong(), C.c_int(), D()

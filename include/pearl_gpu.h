@@ -194,6 +194,36 @@ int pearl_gpu_maybe_shift(pearl_gpu_ctx* ctx, double shift_trigger, double shift
 int pearl_gpu_snapshot(pearl_gpu_ctx* ctx, pearl_diag* out);
 
 /* ---- initialisation on the device (pearl::initialize, pearl_serial.cpp:1761-1837) ---- */
+/* One filling command of the input file (parse_filling_operation,
+ * pearl_serial.cpp:1197-1233): its method and its numeric parameters in input
+ * order, already validated as validate_filling_operations (:1235-1349) does. */
+enum {
+    PEARL_FILL_CUBE = 1,                   /* FILLCUBE, 7 parameters */
+    PEARL_FILL_CYLINDER = 2,               /* FILLCYLINDER, 6 */
+    PEARL_FILL_CENTER_BOX_2D = 3,          /* FILLCENTERBOX2D, 6 */
+    PEARL_FILL_Y_JUNCTION_2D = 4,          /* FILLYJUNCTION2D, 13 */
+    PEARL_FILL_Y_JUNCTION_LAMELLAE_2D = 5, /* FILLYJUNCTIONLAMELLAE2D, 16 */
+    PEARL_FILL_ADHERED_PEARLITE_ARM_2D = 6, /* FILLADHEREDPEARLITEARM2D, 11 */
+    PEARL_FILL_PEARLITE_ELLIPSE_2D = 7     /* FILLPEARLITEELLIPSE2D, 11 */
+};
+#define PEARL_FILL_MAX_PARAMS 16
+#define PEARL_FILL_MAX_OPS 256
+typedef struct pearl_fill_op {
+    int method; /* PEARL_FILL_* */
+    int nparams;
+    double p[PEARL_FILL_MAX_PARAMS];
+} pearl_fill_op;
+/* The "microsim" initial phases on the device: filling_phase_at
+ * (pearl_serial.cpp:1393-1514) of every cell, the commands applied in input
+ * order to a gamma background, written as one-hot phase fractions into the
+ * context's current phase fields (carbon and mu are left as they are; the
+ * step-energy carry is dropped).  The cosine and sine of every command's
+ * angles are taken on the host with the reference's expressions; the cells'
+ * arithmetic runs on the device in the reference's operation order.  Replaces
+ * the host loop over cells of initialize (:1771-1772).  At most
+ * PEARL_FILL_MAX_OPS commands; PEARL_ERR_INVALID_ARGUMENT for an unknown
+ * method or a wrong parameter count. */
+int pearl_gpu_fill(pearl_gpu_ctx* ctx, const pearl_fill_op* ops, int nops);
 /* Capillarity-only smoothing of the current phase fields
  * (smooth_interface_only, pearl_serial.cpp:869-958). */
 int pearl_gpu_smooth_interface(pearl_gpu_ctx* ctx, int max_steps, int min_steps, double energy_rtol,
@@ -226,6 +256,12 @@ const char* pearl_gpu_last_error(const pearl_gpu_ctx* ctx);
 /* Device kernels launched by this context since creation; the grid size of the
  * persistent kernel; the device time of the last launch in milliseconds. */
 int pearl_gpu_stats(const pearl_gpu_ctx* ctx, long long* kernel_launches, int* grid_blocks, double* last_kernel_ms);
+/* Which block owns which cells, the only thing besides the reference's
+ * arithmetic that a result depends on (the order of its global sums): warps
+ * per block (8 or 16; a tile is 32 << warps_x_log2 cells wide and
+ * 2*warps >> warps_x_log2 rows high), and the blocks of the persistent grid
+ * (tile t belongs to block t mod grid_blocks).  No reference counterpart. */
+int pearl_gpu_geometry(const pearl_gpu_ctx* ctx, int* warps, int* warps_x_log2, int* grid_blocks);
 /* Device time of the last launch split by phase (16 slots, milliseconds and
  * phase counts): 0 propose, 1 diffusion set-up, 2 CG apply, 3 CG update,
  * 4 unused (the true-residual recheck runs inside slot 6), 5 CG restart,

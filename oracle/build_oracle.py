@@ -51,8 +51,10 @@ def build_port(force: bool = False) -> Path:
     adj = HERE / "pearl_adjoint.c"
     hdr = HERE / "pearl_oracle.h"
     if force or _stale(ORACLE_SO, src, adj, hdr):
-        _run(["gcc", "-std=c99", "-O3", "-ffp-contract=off", "-fPIC", "-shared", "-Wall", "-Wextra", "-Wno-maybe-uninitialized",
-              str(src), str(adj), "-o", str(ORACLE_SO), "-lm"])
+        # -fopenmp: the device-order mode runs its per-cell loops on host threads
+        # (off by default; results do not depend on the thread count)
+        _run(["gcc", "-std=c99", "-O3", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-Wall", "-Wextra",
+              "-Wno-maybe-uninitialized", str(src), str(adj), "-o", str(ORACLE_SO), "-lm"])
     return ORACLE_SO
 
 

@@ -27,6 +27,94 @@ static inline size_t at(int x, int y, int nx) { return (size_t)y * (size_t)nx + 
 
 static double pi_value(void) { return acos(-1.0); }
 
+/* ---- the device's summation order (pearl_oracle.h, po_set_device_order) ----
+ * Off by default: every function below then sums in the reference's
+ * sequential row-major order.  The per-cell loops that carry no sum run on
+ * g_threads host threads in this mode; their results do not depend on it. */
+static int g_dev = 0;
+static po_device_order g_ord;
+static int g_threads = 1;
+#define DEV_PARALLEL_FOR _Pragma("omp parallel for num_threads(g_threads) if(g_dev && g_threads > 1) schedule(static)")
+
+/* the device's step-energy carry: energy and carbon mass of the last accepted trial */
+static struct {
+    int valid;
+    double e0, mass0;
+} g_carry;
+
+void po_set_device_order(const po_device_order* o) {
+    g_carry.valid = 0;
+    if (!o) {
+        g_dev = 0;
+        g_threads = 1;
+        return;
+    }
+    g_ord = *o;
+    if (g_ord.warps != 16) g_ord.warps = 8;
+    if (g_ord.warps_x_log2 < 0 || (1 << g_ord.warps_x_log2) > g_ord.warps) g_ord.warps_x_log2 = 0;
+    if (g_ord.blocks < 1) g_ord.blocks = 1;
+    g_threads = o->threads > 1 ? o->threads : 1;
+    g_dev = 1;
+}
+
+/* A warp's shuffle-down tree over its 32 lanes: at offsets 16, 8, 4, 2, 1
+ * lane i adds lane i + o; the warp's value is lane 0's. */
+static double lanes_tree(double a[32]) {
+    for (int o = 16; o > 0; o >>= 1)
+        for (int i = 0; i < o; ++i) a[i] = a[i] + a[i + o];
+    return a[0];
+}
+
+double po_device_sum(int nx, int ny, const double* v, int reverse) {
+    const int W = g_ord.warps, wx = g_dev ? g_ord.warps_x_log2 : 0, G = g_dev ? g_ord.blocks : 1;
+    const int tile_w = 32 << wx, tile_h = (2 * W) >> wx;
+    const int ntx = (nx + tile_w - 1) / tile_w, nty = (ny + tile_h - 1) / tile_h, ntiles = ntx * nty;
+    double* part = (double*)malloc(sizeof(double) * (size_t)G);
+    if (!part) return NAN;
+#pragma omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(dynamic, 4)
+    for (int b = 0; b < G; ++b) {
+        /* block b owns tiles b, b+G, ...; each thread keeps one running sum over them */
+        const int nb = b < ntiles ? (ntiles - 1 - b) / G + 1 : 0;
+        double block = 0;
+        for (int w = 0; w < W; ++w) {
+            const int wxi = w & ((1 << wx) - 1), wy = w >> wx;
+            double lanes[32];
+            for (int l = 0; l < 32; ++l) {
+                double acc = 0;
+                for (int k = 0; k < nb; ++k) {
+                    const int t = b + (reverse ? nb - 1 - k : k) * G;
+                    const int x = (t % ntx) * tile_w + (wxi << 5) + l, y0 = (t / ntx) * tile_h + 2 * wy;
+                    if (x < nx && y0 < ny) {
+                        acc += v[(size_t)y0 * (size_t)nx + (size_t)x];
+                        if (y0 + 1 < ny) acc += v[(size_t)(y0 + 1) * (size_t)nx + (size_t)x];
+                    }
+                }
+                lanes[l] = acc;
+            }
+            const double wv = lanes_tree(lanes);
+            block = w == 0 ? wv : block + wv; /* warps in index order */
+        }
+        part[b] = block;
+    }
+    /* 32 lanes add the block partials strided by 32, then one more tree */
+    double lanes[32];
+    for (int l = 0; l < 32; ++l) {
+        double acc = 0;
+        for (int b = l; b < G; b += 32) acc += part[b];
+        lanes[l] = acc;
+    }
+    free(part);
+    return lanes_tree(lanes);
+}
+
+/* the device's dot product: per-cell products, then its tree */
+static double device_dot(const double* a, const double* b, double* prod, int nx, int ny, int reverse) {
+    const size_t n = (size_t)nx * (size_t)ny;
+    DEV_PARALLEL_FOR
+    for (long long i = 0; i < (long long)n; ++i) prod[i] = a[i] * b[i];
+    return po_device_sum(nx, ny, prod, reverse);
+}
+
 /* Parabola::psi, pearl_serial.cpp:86-89 */
 double po_psi(const po_params* p, int phase, double mu) {
     const double d = mu - p->B[phase];
@@ -112,15 +200,75 @@ static inline void load3(const double* phi, int x, int y, int nx, double v[3]) {
 
 /* total_carbon, pearl_serial.cpp:784-788 */
 double po_total_carbon(const po_params* p, int nx, int ny, const double* carbon) {
+    if (g_dev) return po_device_sum(nx, ny, carbon, 0) * p->dx * p->dy; /* step-start order */
     double v = 0;
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x) v += carbon[at(x, y, nx)];
     return v * p->dx * p->dy;
 }
 
+/* reduced_energy's density per cell as the device sums it (pearl_serial.cpp:800-819):
+ * the cell's chemical, obstacle and triple terms, then its +x and +y face terms
+ * added to that cell's value.  cell[] receives nx*ny values; returns
+ * PO_ERR_MIXTURE where the reference throws. */
+static int energy_cells_device(const po_params* p, int nx, int ny, const double* phi, const double* carbon,
+                               double* cell) {
+    const double eps = p->epsilon, sigma = p->sigma;
+    const double pi = pi_value();
+    const double obstacle = 16 * sigma / (pi * pi * eps), triple = p->triple / eps;
+    const double mu_r = p->mu_reference;
+    const double psi[3] = {po_psi(p, 0, mu_r) - po_psi(p, 2, mu_r), po_psi(p, 1, mu_r) - po_psi(p, 2, mu_r), 0};
+    int bad = 0;
+#pragma omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static) reduction(|:bad)
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) {
+            double q[3], h[3];
+            load3(phi, x, y, nx, q);
+            po_weights(q, h);
+            double chem = 0;
+            for (int a = 0; a < 3; ++a) chem += h[a] * psi[a];
+            if (!p->phase_only) {
+                double chi, ci, k;
+                if (po_mixture(p, q, &chi, &ci, &k) != PO_OK) bad = 1;
+                const double dc = carbon[at(x, y, nx)] - fma(chi, mu_r, ci);
+                chem += .5 * dc * dc / chi;
+            }
+            double t = chem / p->Vm + obstacle * (q[0] * q[1] + q[0] * q[2] + q[1] * q[2]) + triple * q[0] * q[1] * q[2];
+            for (int dir = 0; dir < 2; ++dir) {
+                if (dir == 1 && y == ny - 1) continue;
+                double nb[3];
+                if (dir == 0)
+                    load3(phi, xp(x, nx), y, nx, nb);
+                else
+                    load3(phi, x, y + 1, nx, nb);
+                const double dist = dir == 0 ? p->dx : p->dy;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = a + 1; b < 3; ++b) {
+                        const double z = (q[a] * nb[b] - nb[a] * q[b]) / dist;
+                        t += eps * sigma * z * z;
+                    }
+            }
+            cell[at(x, y, nx)] = t;
+        }
+    return bad ? PO_ERR_MIXTURE : PO_OK;
+}
+
+/* reduced_energy in the device's order: the step-start pass walks forwards,
+ * the final update of a step backwards */
+static int reduced_energy_device(const po_params* p, int nx, int ny, const double* phi, const double* carbon,
+                                 int reverse, double* energy) {
+    double* cell = (double*)malloc(sizeof(double) * (size_t)nx * (size_t)ny);
+    if (!cell) return PO_ERR_INVALID_ARGUMENT;
+    const int rc = energy_cells_device(p, nx, ny, phi, carbon, cell);
+    if (rc == PO_OK) *energy = po_device_sum(nx, ny, cell, reverse) * p->dx * p->dy;
+    free(cell);
+    return rc;
+}
+
 /* reduced_energy, pearl_serial.cpp:793-821 */
 int po_reduced_energy(const po_params* p, int nx, int ny, const double* phi, const double* carbon,
                       double* energy) {
+    if (g_dev) return reduced_energy_device(p, nx, ny, phi, carbon, 0, energy);
     const double eps = p->epsilon, sigma = p->sigma;
     const double pi = pi_value();
     const double obstacle = 16 * sigma / (pi * pi * eps), triple = p->triple / eps;
@@ -160,62 +308,92 @@ int po_reduced_energy(const po_params* p, int nx, int ny, const double* phi, con
     return PO_OK;
 }
 
-/* propose_phi, pearl_serial.cpp:961-1002 */
+/* propose_phi for the cell (x, y), pearl_serial.cpp:966-1001: writes the trial
+ * phase fractions and *change = max |dphi| of the cell (INFINITY, with the old
+ * fractions kept, where the proposal is not finite, :990-996). */
+static int propose_cell(const po_params* p, int nx, int ny, const double* phi_old, const double* mu_old,
+                        double* trial_phi, double dt, double obs, double tr, int x, int y, double* change) {
+    static const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+    const double eps = p->epsilon, sigma = p->sigma;
+    double q[3], force[3] = {0, 0, 0}, dh[3][3];
+    load3(phi_old, x, y, nx, q);
+    const double mu = mu_old[at(x, y, nx)];
+    const double psi0 = po_psi(p, 2, mu);
+    po_weight_derivatives(q, dh);
+    for (int a = 0; a < 3; ++a) {
+        force[a] = obs * (q[(a + 1) % 3] + q[(a + 2) % 3]) + tr * q[(a + 1) % 3] * q[(a + 2) % 3];
+        for (int b = 0; b < 3; ++b) force[a] += (po_psi(p, b, mu) - psi0) * dh[b][a] / p->Vm;
+    }
+    for (int dir = 0; dir < 4; ++dir) {
+        if ((dir == 2 && y == 0) || (dir == 3 && y == ny - 1)) continue;
+        int xx = x, yy = y;
+        if (ox[dir] < 0) xx = xm(x, nx);
+        if (ox[dir] > 0) xx = xp(x, nx);
+        if (oy[dir] < 0) yy = ym(y);
+        if (oy[dir] > 0) yy = yp(y, ny);
+        double nb[3];
+        load3(phi_old, xx, yy, nx, nb);
+        const double dist = dir < 2 ? p->dx : p->dy;
+        for (int a = 0; a < 3; ++a)
+            for (int b = a + 1; b < 3; ++b) {
+                const double w = 2 * eps * sigma * (q[a] * nb[b] - nb[a] * q[b]) / (dist * dist);
+                force[a] += w * nb[b];
+                force[b] -= w * nb[a];
+            }
+    }
+    const double mean = (force[0] + force[1] + force[2]) / 3, scale = dt / (po_local_tau(q, p->tau) * eps);
+    double z[3];
+    for (int a = 0; a < 3; ++a) z[a] = q[a] - scale * (force[a] - mean);
+    int finite = 1;
+    for (int a = 0; a < 3; ++a) finite = finite && isfinite(z[a]);
+    double* out = trial_phi + at(x, y, nx) * 3;
+    if (!finite) {
+        *change = INFINITY;
+        out[0] = q[0];
+        out[1] = q[1];
+        out[2] = q[2];
+        return PO_OK;
+    }
+    double zp[3];
+    if (po_project_simplex(z, zp) != PO_OK) return PO_ERR_SIMPLEX;
+    double c = 0;
+    for (int a = 0; a < 3; ++a) c = dmax(c, fabs(zp[a] - q[a]));
+    *change = c;
+    out[0] = zp[0];
+    out[1] = zp[1];
+    out[2] = zp[2];
+    return PO_OK;
+}
+
+/* propose_phi, pearl_serial.cpp:961-1002.  The global max |dphi| is the same
+ * in any cell order; in the device's order the rows run on host threads. */
 int po_propose_phi(const po_params* p, int nx, int ny, const double* phi_old, const double* mu_old,
                    double* trial_phi, double dt, double* change_out) {
     const double eps = p->epsilon, sigma = p->sigma;
     const double pi = pi_value();
     const double obs = 16 * sigma / (pi * pi * eps), tr = p->triple / eps;
     double change = 0;
-    static const int ox[4] = {-1, 1, 0, 0}, oy[4] = {0, 0, -1, 1};
+    if (g_dev) {
+        int bad = 0;
+#pragma omp parallel for num_threads(g_threads) if(g_threads > 1) schedule(static) reduction(max:change) reduction(|:bad)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                double c;
+                if (propose_cell(p, nx, ny, phi_old, mu_old, trial_phi, dt, obs, tr, x, y, &c) != PO_OK)
+                    bad = 1;
+                else
+                    change = c > change ? c : change;
+            }
+        if (bad) return PO_ERR_SIMPLEX;
+        *change_out = change;
+        return PO_OK;
+    }
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x) {
-            double q[3], force[3] = {0, 0, 0}, dh[3][3];
-            load3(phi_old, x, y, nx, q);
-            const double mu = mu_old[at(x, y, nx)];
-            const double psi0 = po_psi(p, 2, mu);
-            po_weight_derivatives(q, dh);
-            for (int a = 0; a < 3; ++a) {
-                force[a] = obs * (q[(a + 1) % 3] + q[(a + 2) % 3]) + tr * q[(a + 1) % 3] * q[(a + 2) % 3];
-                for (int b = 0; b < 3; ++b) force[a] += (po_psi(p, b, mu) - psi0) * dh[b][a] / p->Vm;
-            }
-            for (int dir = 0; dir < 4; ++dir) {
-                if ((dir == 2 && y == 0) || (dir == 3 && y == ny - 1)) continue;
-                int xx = x, yy = y;
-                if (ox[dir] < 0) xx = xm(x, nx);
-                if (ox[dir] > 0) xx = xp(x, nx);
-                if (oy[dir] < 0) yy = ym(y);
-                if (oy[dir] > 0) yy = yp(y, ny);
-                double nb[3];
-                load3(phi_old, xx, yy, nx, nb);
-                const double dist = dir < 2 ? p->dx : p->dy;
-                for (int a = 0; a < 3; ++a)
-                    for (int b = a + 1; b < 3; ++b) {
-                        const double w = 2 * eps * sigma * (q[a] * nb[b] - nb[a] * q[b]) / (dist * dist);
-                        force[a] += w * nb[b];
-                        force[b] -= w * nb[a];
-                    }
-            }
-            const double mean = (force[0] + force[1] + force[2]) / 3,
-                         scale = dt / (po_local_tau(q, p->tau) * eps);
-            double z[3];
-            for (int a = 0; a < 3; ++a) z[a] = q[a] - scale * (force[a] - mean);
-            int finite = 1;
-            for (int a = 0; a < 3; ++a) finite = finite && isfinite(z[a]);
-            double* out = trial_phi + at(x, y, nx) * 3;
-            if (!finite) {
-                change = INFINITY;
-                out[0] = q[0];
-                out[1] = q[1];
-                out[2] = q[2];
-                continue;
-            }
-            double zp[3];
-            if (po_project_simplex(z, zp) != PO_OK) return PO_ERR_SIMPLEX;
-            for (int a = 0; a < 3; ++a) change = dmax(change, fabs(zp[a] - q[a]));
-            out[0] = zp[0];
-            out[1] = zp[1];
-            out[2] = zp[2];
+            double c;
+            if (propose_cell(p, nx, ny, phi_old, mu_old, trial_phi, dt, obs, tr, x, y, &c) != PO_OK)
+                return PO_ERR_SIMPLEX;
+            change = dmax(change, c);
         }
     *change_out = change;
     return PO_OK;
@@ -236,6 +414,7 @@ static inline void face_weights(const po_params* p, const double* K, int x, int 
 /* apply, pearl_serial.cpp:1029-1035 */
 static void apply_op(const po_params* p, const double* K, const double* chi, double dt, int nx, int ny,
                      const double* in, double* out) {
+    DEV_PARALLEL_FOR
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x) {
             double w[4];
@@ -255,29 +434,42 @@ static double dot(const double* a, const double* b, size_t n) {
 }
 
 /* implicit_diffusion, pearl_serial.cpp:1010-1094.  u_out (may be NULL) receives
- * the converged solution u = mu - mu_reference of the linear system. */
+ * the converged solution u = mu - mu_reference of the linear system.
+ *
+ * In the device's order (po_set_device_order) every dot product is the
+ * device's tree over the same per-cell products, walked as the device's pass
+ * that forms it: the set-up sums (rhs.rhs, r.z, r.r), the CG update's (r.z,
+ * r.r) and the restart's r.z forwards, the apply's p.Ap and the true residual's
+ * r.r backwards; the residual tested at the head of an iteration is the r.r of
+ * the pass that last wrote r, which is what the reference recomputes there. */
 int po_implicit_diffusion_u(const po_params* p, int nx, int ny, const double* carbon_old, const double* mu_old,
                             const double* trial_phi, double* trial_carbon, double* trial_mu, double dt,
                             po_diffusion_info* info, double* u_out) {
     const size_t n = (size_t)nx * (size_t)ny;
+    const long long nn = (long long)n;
     const double mu_r = p->mu_reference;
-    double* mem = (double*)malloc(sizeof(double) * n * 10);
+    double* mem = (double*)malloc(sizeof(double) * n * 11);
     if (!mem) return PO_ERR_INVALID_ARGUMENT;
     double *chi = mem, *icpt = mem + n, *K = mem + 2 * n, *rhs = mem + 3 * n, *u = mem + 4 * n, *diag = mem + 5 * n;
-    double *r = mem + 6 * n, *z = mem + 7 * n, *pd = mem + 8 * n, *Ap = mem + 9 * n;
-    for (size_t i = 0; i < n; ++i) {
+    double *r = mem + 6 * n, *z = mem + 7 * n, *pd = mem + 8 * n, *Ap = mem + 9 * n, *prod = mem + 10 * n;
+#define PO_DOT(a, b, reverse) (g_dev ? device_dot(a, b, prod, nx, ny, reverse) : dot(a, b, n))
+    int mixbad = 0;
+#pragma omp parallel for num_threads(g_threads) if(g_dev && g_threads > 1) schedule(static) reduction(|:mixbad)
+    for (long long i = 0; i < nn; ++i) {
         double c, ci, k;
-        if (po_mixture(p, trial_phi + 3 * i, &c, &ci, &k) != PO_OK) {
-            free(mem);
-            return PO_ERR_MIXTURE;
-        }
+        if (po_mixture(p, trial_phi + 3 * i, &c, &ci, &k) != PO_OK) mixbad = 1;
         chi[i] = c;
         icpt[i] = fma(c, mu_r, ci);
         K[i] = k;
         rhs[i] = carbon_old[i] - icpt[i];
         u[i] = mu_old[i] - mu_r;
     }
+    if (mixbad) {
+        free(mem);
+        return PO_ERR_MIXTURE;
+    }
     apply_op(p, K, chi, dt, nx, ny, u, Ap);
+    DEV_PARALLEL_FOR
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x) {
             double w[4];
@@ -288,12 +480,13 @@ int po_implicit_diffusion_u(const po_params* p, int nx, int ny, const double* ca
             z[i] = r[i] / diag[i];
             pd[i] = z[i];
         }
-    const double tolerance = p->cg_atol + p->cg_rtol * sqrt(dot(rhs, rhs, n));
-    double rz = dot(r, z, n);
+    const double tolerance = p->cg_atol + p->cg_rtol * sqrt(PO_DOT(rhs, rhs, 0));
+    double rz = PO_DOT(r, z, 0);
+    double rr = g_dev ? PO_DOT(r, r, 0) : 0; /* the device's r.r of the pass that last wrote r */
     po_diffusion_info inf = {0, 0, 0.0, 0.0};
     for (int iteration = 0; iteration <= p->cg_max; ++iteration) {
         inf.it = iteration;
-        inf.residual = sqrt(dot(r, r, n));
+        inf.residual = sqrt(g_dev ? rr : dot(r, r, n));
         if (!isfinite(inf.residual)) {
             *info = inf;
             free(mem);
@@ -301,43 +494,51 @@ int po_implicit_diffusion_u(const po_params* p, int nx, int ny, const double* ca
         }
         if (inf.residual <= tolerance) {
             apply_op(p, K, chi, dt, nx, ny, u, Ap);
-            for (size_t i = 0; i < n; ++i) r[i] = rhs[i] - Ap[i];
-            inf.residual = sqrt(dot(r, r, n));
+            DEV_PARALLEL_FOR
+            for (long long i = 0; i < nn; ++i) r[i] = rhs[i] - Ap[i];
+            rr = PO_DOT(r, r, 1);
+            inf.residual = sqrt(rr);
             if (inf.residual <= tolerance * 1.05) {
                 inf.ok = 1;
                 break;
             }
-            for (size_t i = 0; i < n; ++i) {
+            DEV_PARALLEL_FOR
+            for (long long i = 0; i < nn; ++i) {
                 z[i] = r[i] / diag[i];
                 pd[i] = z[i];
             }
-            rz = dot(r, z, n);
+            rz = PO_DOT(r, z, 0);
             continue;
         }
         if (iteration == p->cg_max) break;
         apply_op(p, K, chi, dt, nx, ny, pd, Ap);
-        const double pAp = dot(pd, Ap, n);
+        const double pAp = PO_DOT(pd, Ap, 1);
         if (!(pAp > 0) || !isfinite(pAp) || !isfinite(rz)) {
             *info = inf;
             free(mem);
             return PO_OK;
         }
         const double alpha = rz / pAp;
-        for (size_t i = 0; i < n; ++i) {
+        DEV_PARALLEL_FOR
+        for (long long i = 0; i < nn; ++i) {
             u[i] += alpha * pd[i];
             r[i] -= alpha * Ap[i];
             z[i] = r[i] / diag[i];
         }
-        const double rz_next = dot(r, z, n), beta = rz_next / rz;
+        const double rz_next = PO_DOT(r, z, 0), beta = rz_next / rz;
+        if (g_dev) rr = PO_DOT(r, r, 0);
         rz = rz_next;
-        for (size_t i = 0; i < n; ++i) pd[i] = z[i] + beta * pd[i];
+        DEV_PARALLEL_FOR
+        for (long long i = 0; i < nn; ++i) pd[i] = z[i] + beta * pd[i];
     }
+#undef PO_DOT
     if (!inf.ok) {
         *info = inf;
         free(mem);
         return PO_OK;
     }
     double closure = 0;
+#pragma omp parallel for num_threads(g_threads) if(g_dev && g_threads > 1) schedule(static) reduction(max:closure)
     for (int y = 0; y < ny; ++y)
         for (int x = 0; x < nx; ++x) {
             double w[4];
@@ -368,8 +569,9 @@ int po_implicit_diffusion(const po_params* p, int nx, int ny, const double* carb
 int po_valid_state(const po_params* p, int nx, int ny, const double* phi, const double* carbon,
                    const double* mu) {
     int good = 1;
-    const size_t n = (size_t)nx * (size_t)ny;
-    for (size_t i = 0; i < n; ++i) {
+    const long long n = (long long)nx * (long long)ny;
+#pragma omp parallel for num_threads(g_threads) if(g_dev && g_threads > 1) schedule(static) reduction(&&:good)
+    for (long long i = 0; i < n; ++i) {
         double sum = 0;
         const double* q = phi + 3 * i;
         for (int a = 0; a < 3; ++a) {
@@ -398,12 +600,18 @@ int po_advance(const po_params* p, int nx, int ny, double* phi, double* carbon, 
     if (stop_time - s->time < dt) dt = stop_time - s->time;
     if (!(dt > 0) || !isfinite(dt)) return PO_ERR_INVALID_ADVANCE_TIME;
     const size_t n = (size_t)nx * (size_t)ny;
-    double e0 = 0;
-    if (p->check_energy) {
-        int rc = po_reduced_energy(p, nx, ny, phi, carbon, &e0);
-        if (rc) return rc;
+    double e0 = 0, mass0 = 0;
+    if (g_dev && g_carry.valid) {
+        /* the device carries the accepted trial's energy and mass into the next step */
+        e0 = g_carry.e0;
+        mass0 = g_carry.mass0;
+    } else {
+        if (p->check_energy) {
+            int rc = po_reduced_energy(p, nx, ny, phi, carbon, &e0);
+            if (rc) return rc;
+        }
+        mass0 = p->phase_only ? 0 : po_total_carbon(p, nx, ny, carbon);
     }
-    const double mass0 = p->phase_only ? 0 : po_total_carbon(p, nx, ny, carbon);
     int why = PO_WHY_NONE;
     double* tphi = (double*)malloc(sizeof(double) * n * 5);
     if (!tphi) return PO_ERR_INVALID_ARGUMENT;
@@ -452,14 +660,17 @@ int po_advance(const po_params* p, int nx, int ny, double* phi, double* carbon, 
             good = po_valid_state(p, nx, ny, tphi, tc, tmu);
             why = PO_WHY_BOUNDS;
         }
+        /* in the device's order the trial's mass and energy are sums of its final
+         * update, which walks backwards (phase-only: its energy pass, forwards) */
+        double m = 0, e1 = 0;
         if (good && !p->phase_only) {
-            const double m = po_total_carbon(p, nx, ny, tc);
+            m = g_dev ? po_device_sum(nx, ny, tc, 1) * p->dx * p->dy : po_total_carbon(p, nx, ny, tc);
             good = fabs(m - mass0) <= 1e-11 * dmax(fabs(mass0), gxgy * p->dx * p->dy * 1e-6);
             why = PO_WHY_MASS;
         }
         if (good && p->check_energy) {
-            double e1;
-            rc = po_reduced_energy(p, nx, ny, tphi, tc, &e1);
+            rc = g_dev ? reduced_energy_device(p, nx, ny, tphi, tc, !p->phase_only, &e1)
+                       : po_reduced_energy(p, nx, ny, tphi, tc, &e1);
             if (rc) {
                 free(tphi);
                 return rc;
@@ -478,6 +689,11 @@ int po_advance(const po_params* p, int nx, int ny, double* phi, double* carbon, 
             s->step = s->step + 1;
             s->rejected = s->rejected + attempt;
             s->dt = dmin(p->dt_max, dt * 1.1);
+            if (g_dev) {
+                g_carry.valid = 1;
+                g_carry.e0 = p->check_energy ? e1 : 0;
+                g_carry.mass0 = p->phase_only ? 0 : m;
+            }
             if (out_info) *out_info = out;
             if (why_out) *why_out = PO_WHY_NONE;
             free(tphi);
@@ -499,6 +715,7 @@ int po_advance_n(const po_params* p, int nx, int ny, double* phi, double* carbon
                  int nsteps, const double* forced_dt, double stop_time, po_step_info* infos, int* why,
                  int* steps_done) {
     int done = 0, rc = PO_OK;
+    g_carry.valid = 0; /* a run starts from the given fields: no carried energy */
     for (int k = 0; k < nsteps; ++k) {
         if (forced_dt) s->dt = forced_dt[k];
         rc = po_advance(p, nx, ny, phi, carbon, mu, s, stop_time, infos ? infos + k : NULL, why);

@@ -84,6 +84,39 @@ enum {
     PO_WHY_ENERGY = 5
 };
 
+/* ---- summation order of the device kernels ----
+ * The reference sums every global quantity sequentially in row-major order
+ * (Domain::sum, pearl_serial.cpp:649-666; array_dot, :738-742; total_carbon,
+ * :784-788; reduced_energy, :793-821).  libpearl_gpu sums the same per-cell
+ * values in a fixed tree instead: the grid's blocks own tiles of 32 x 2*warps
+ * cells (tile t: column t % ntx, row t / ntx; block b owns t = b, b+blocks,
+ * ...), each thread accumulates its two cells (x, y0) and (x, y0+1) over its
+ * block's tiles in the pass's walk order, warps reduce by shuffles
+ * (offsets 16, 8, 4, 2, 1), a block adds its warps in index order, and 32
+ * lanes add the block partials strided by 32 before a last shuffle tree.
+ * Passes walk their tiles forwards (set-up, CG update, restart, step-start
+ * energy) or backwards (CG apply, final update with its mass and energy), and
+ * the energy of a cell is summed per cell first (cell terms, then its faces).
+ * The device also carries the accepted trial's energy and carbon mass into
+ * the next step instead of recomputing them.
+ *
+ * po_set_device_order(o) makes this oracle follow that order and that carry
+ * (per-cell arithmetic is unchanged), so that, given the device's grid, it
+ * reproduces the device's results bit for bit; po_set_device_order(NULL)
+ * restores the reference's order.  o->threads > 1 runs the per-cell loops of
+ * that mode on host threads (the results do not depend on it).  Test
+ * infrastructure: it shows that the device differs from the reference only
+ * in the order of its sums. */
+typedef struct po_device_order {
+    int warps;         /* warps per block: 8 (32x16 tiles) or 16 (32x32 tiles) */
+    int warps_x_log2;  /* warps side by side in x: the tile is (32 << w) x (2*warps >> w) cells */
+    int blocks;        /* blocks in the grid */
+    int threads;       /* host threads for the per-cell loops */
+} po_device_order;
+void po_set_device_order(const po_device_order* order);
+/* The device's tree sum of v[y*nx + x] over the domain; reverse = walk order. */
+double po_device_sum(int nx, int ny, const double* v, int reverse);
+
 /* ---- pointwise thermodynamics (pearl_serial.cpp:76-145) ---- */
 double po_psi(const po_params* p, int phase, double mu);
 void po_weights(const double phi[3], double h[3]);

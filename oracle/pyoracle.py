@@ -66,6 +66,10 @@ class PoDiag(C.Structure):
     _fields_ = [(n, D) for n in ("c_min", "c_max", "mu_min", "mu_max", "phi_sum_error", "mass", "ledger", "energy")]
 
 
+class PoDeviceOrder(C.Structure):
+    _fields_ = [("warps", C.c_int), ("warps_x_log2", C.c_int), ("blocks", C.c_int), ("threads", C.c_int)]
+
+
 class PoSmoothReport(C.Structure):
     _fields_ = [
         ("steps", C.c_int), ("converged", C.c_int),
@@ -142,12 +146,49 @@ class Port(_Lib):
         L.po_interface_energy_only.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP]
         L.po_interface_energy_only.restype = D
         L.po_close_mu.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP]
+        L.po_set_device_order.argtypes = [C.POINTER(PoDeviceOrder)]
+        L.po_set_device_order.restype = None
+        L.po_device_sum.argtypes = [C.c_int, C.c_int, DP, C.c_int]
+        L.po_device_sum.restype = D
         L.po_psi.argtypes = [C.POINTER(PoParams), C.c_int, D]
         L.po_psi.restype = D
         L.po_adjoint_gradient.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP, C.POINTER(PoScalars),
                                           C.c_int, C.c_int, DP, C.POINTER(PoAdjointReport)]
         L.po_adjoint_objective.argtypes = [C.POINTER(PoParams), C.c_int, C.c_int, DP, DP, DP,
                                            C.POINTER(PoScalars), C.c_int, DP, DP]
+
+    def set_device_order(self, warps: int | None, blocks: int = 1, warps_x_log2: int = 0,
+                         threads: int | None = None) -> None:
+        """Sum in libpearl_gpu's tree order for a grid of `blocks` blocks of
+        `warps` warps (see pearl_oracle.h); warps=None restores the reference's
+        sequential order."""
+        if warps is None:
+            self.lib.po_set_device_order(None)
+            return
+        import os
+
+        o = PoDeviceOrder(warps, warps_x_log2, blocks, threads if threads else (os.cpu_count() or 1))
+        self.lib.po_set_device_order(C.byref(o))
+
+    def device_order(self, warps: int, blocks: int, warps_x_log2: int = 0, threads: int | None = None):
+        """Context manager: the device's summation order inside, the reference's after."""
+        import contextlib
+
+        @contextlib.contextmanager
+        def _cm():
+            self.set_device_order(warps, blocks, warps_x_log2, threads)
+            try:
+                yield self
+            finally:
+                self.set_device_order(None)
+
+        return _cm()
+
+    def device_sum(self, v, reverse: bool = False) -> float:
+        """The device's tree sum of v[ny, nx] under the current device order."""
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        ny, nx = v.shape
+        return self.lib.po_device_sum(nx, ny, _p(v), int(reverse))
 
     def psi(self, params, phase: int, mu: float) -> float:
         return self.lib.po_psi(C.byref(_params(params)), phase, mu)

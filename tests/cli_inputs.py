@@ -98,6 +98,45 @@ def case_smoke():
         ("smooth_energy_rtol", "1e-10"), ("smooth_max_phase_change", "0.02")]
 
 
+# Filling commands of every method, on the 137x250 grid of the reference's
+# examples (values chosen off the grid lines, angles off the axes, so that the
+# cells near the painted boundaries test the arithmetic).
+FILL_CASES = {
+    # the reference's G137 sharp geometry: 17 theta and 120 alpha columns in rows 0..20
+    "cube_g137": [("FILLCUBE", "{1,0,0,0,16,20,0};"), ("FILLCUBE", "{0,17,0,0,136,20,0};")],
+    "cylinders": [("FILLCYLINDER", "{0,68,125,0,0,40.5}"), ("FILLCYLINDER", "{1,68,125,0,0,13.7}"),
+                  ("FILLCYLINDER", "{0,20,200,0,0,9}")],
+    "center_box": [("FILLCENTERBOX2D", "{10,127,30,220,1,0}"), ("FILLCUBE", "{2,0,0,0,5,5,0}"),
+                   ("FILLCUBE", "{1,60,100,0,70,140,0}")],
+    "y_junction": [("FILLYJUNCTION2D", "{0,137,0,250,68,125,90,210,330,120,14.5,0,2}")],
+    "y_junction_lamellae": [("FILLYJUNCTIONLAMELLAE2D", "{5,130,10,240,70,120,17,137,257,110,20,7.3,1.9,0,1,2}")],
+    "adhered_arm": [("FILLADHEREDPEARLITEARM2D", "{12.5,30,63.4,160,9,0.125,6.5,2.25,4,0,1}")],
+    "adhered_arm_steep": [("FILLADHEREDPEARLITEARM2D", "{120.25,10.5,121.7,180,14,0.2,5.5,0,0,1,0}")],
+    "ellipse": [("FILLPEARLITEELLIPSE2D", "{68.5,20.25,77,10,12,14.2,0.35,0.13,5,0,1}")],
+    "ellipse_rotated": [("FILLPEARLITEELLIPSE2D", "{30,200,-33.3,0,7,11.1,0.6,0.3,0,1,0}")],
+    "sequence": [("FILLCENTERBOX2D", "{0,137,0,250,0,2}"),
+                 ("FILLYJUNCTION2D", "{20,120,40,200,70,120,45,165,285,90,8.5,1,2}"),
+                 ("FILLCYLINDER", "{0,70,120,0,0,6.25}"),
+                 ("FILLADHEREDPEARLITEARM2D", "{70,120,-90,100,5,0.3,4,1.5,3.5,1,0}"),
+                 ("FILLPEARLITEELLIPSE2D", "{100,60,15,2,5,9.7,0.5,0.2,2,0,1}"),
+                 ("FILLCUBE", "{1,130,240,0,136,249,0}")],
+}
+
+
+def case_fill(name: str):
+    """A microsim input painting FILL_CASES[name] on 137x250 (one smoothing step)."""
+    return PHASE_DIAGRAM_10K + grid(137, 250) + COMMON + [
+        ("initialization", "microsim"), *FILL_CASES[name], ("gamma_carbon", "0.034458832049305582"),
+        ("smooth_steps", "1"), ("smooth_min_steps", "1")]
+
+
+def fill_params(value: str) -> list[float]:
+    """The numbers of a filling command's value "{a,b,...};"."""
+    v = value.strip().rstrip(";").strip()
+    assert v[0] == "{" and v[-1] == "}"
+    return [float(t) for t in v[1:-1].split(",")]
+
+
 VALID = {
     "sharp_smooth": case_sharp_smooth,
     "lamella_linear_gp": case_lamella_linear_gp,
