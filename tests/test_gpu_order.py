@@ -145,9 +145,9 @@ def test_small_workload_20000_steps_bitwise_and_drift_is_summation_order(gpu_lib
     _assert_bitwise(gpu, ora, infos, oinfos)
     phi, c, mu, s = gpu
     # the reference took the same decisions at every one of the 20000 steps
-    assert [i.retries for i in infos] == golden["retries"]
-    assert [i.accepted_dt for i in infos] == golden["accepted_dt"]
-    assert [i.cg_iterations for i in infos] == golden["cg_iterations"]
+    assert [i.retries for i in infos] == ref["steps/retries"].tolist()
+    assert [i.accepted_dt for i in infos] == ref["steps/accepted_dt"].tolist()
+    assert [i.cg_iterations for i in infos] == ref["steps/cg_iterations"].tolist()
     rphi, rc_, rmu = ref[f"s{n}/phi"], ref[f"s{n}/carbon"], ref[f"s{n}/mu"]
     assert s.time == ref[f"s{n}/scalars"][0] and s.rejected == ref[f"s{n}/scalars"][3]
     # phi and carbon stay within the FP64 bars after 20000 steps

@@ -195,3 +195,26 @@ def test_port_matches_reference_live(port, reference):
             assert np.array_equal(a, b)
         else:
             assert a == b
+
+
+def test_port_matches_reference_golden_at_config_horizon(port):
+    """The small FP64 configuration at its own horizon: 2000 accepted steps of
+    the C restatement equal the reference's own run (tests/golden/
+    make_horizon_golden.py) bitwise, every step's decisions included (about
+    20 s of CPU)."""
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    ref = np.load(GOLDEN / "horizon_fields.npz")
+    w = workloads.plain_small()
+    phi, c, mu = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    s = pyoracle.scalars_from(w.scalars)
+    rc, why, done, infos = port.advance_n(w.params, phi, c, mu, s, 2000)
+    assert rc == 0 and done == 2000, why
+    assert [i.retries for i in infos] == ref["steps/retries"][:2000].tolist()
+    assert [i.cg_iterations for i in infos] == ref["steps/cg_iterations"][:2000].tolist()
+    assert [i.accepted_dt for i in infos] == ref["steps/accepted_dt"][:2000].tolist()
+    assert np.array_equal(phi, ref["s2000/phi"])
+    assert np.array_equal(c, ref["s2000/carbon"])
+    assert np.array_equal(mu, ref["s2000/mu"])
+    assert (s.time, s.dt, float(s.step), float(s.rejected)) == tuple(ref["s2000/scalars"])
