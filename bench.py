@@ -23,7 +23,8 @@ domain, including rejected attempts.  Metric: cell-updates/s = nx*ny*steps/time.
            source (oracle/_ref), else the C restatement, on host cores.
 
 Other workloads (same JSON contract, not the default line):
-  --precision mixed     the same domain with FP32 propose forces
+  --precision mixed     the same domain in the mixed form: FP32 propose forces and
+                        FP32 inner-solve rounds closed by FP64 residuals
   --workload sweep      256 independent instances in one batched launch, with
                         the autotuner and an all-cores CPU baseline
   --workload adjoint    gradient of a 256x512, --steps-step run w.r.t. mobility,
@@ -77,8 +78,9 @@ def parse_args(argv=None):
     ap.add_argument("--checkpoint-every", type=int, default=50, help="adjoint: steps per checkpoint segment")
     ap.add_argument("--cpu-gradient-steps", type=int, default=100,
                     help="adjoint: steps of the run the CPU reference gradient covers (bounded CPU time)")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
-                    help="fp64 (default): the reference's arithmetic; mixed: FP32 propose forces")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_propose", "mixed_solve"], default="fp64",
+                    help="fp64 (default): the reference's arithmetic; mixed: FP32 propose forces and FP32 "
+                         "inner-solve rounds with FP64 refinement; mixed_propose / mixed_solve: one of the two")
     ap.add_argument("--probe", choices=["propose", "diffusion", "fp64-peak"], default=None,
                     help="profiling aid instead of the bench line: launch one phase of the hot path on its own "
                          "(propose: propose_phi + mixture; diffusion: one proposal, then the implicit solve) "

@@ -61,7 +61,8 @@ extern "C" int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, 
                                           const double* target_alpha, pearl_adjoint_report* out) {
     if (!ctx || nsteps < 1 || checkpoint_every < 1 || !target_alpha || !out) return PEARL_ERR_INVALID_ARGUMENT;
     if (ctx->params.phase_only) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "adjoint needs implicit diffusion");
-    if (ctx->P.mixed) return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "adjoint differentiates the FP64 step");
+    if (ctx->P.mixed || ctx->P.mixed_cg)
+        return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "adjoint differentiates the FP64 step");
     PG_CUDA(ctx, cudaSetDevice(ctx->device));
     std::memset(out, 0, sizeof *out);
     const size_t pe = plane_elems(ctx);

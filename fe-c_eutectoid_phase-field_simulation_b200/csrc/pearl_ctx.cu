@@ -654,6 +654,7 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->d_fill) cudaFree(ctx->d_fill);
+    if (ctx->slab32) cudaFree(ctx->slab32);
     if (ctx->d_hist) cudaFree(ctx->d_hist);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -667,9 +668,30 @@ int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream) {
 }
 
 int pearl_gpu_set_precision(pearl_gpu_ctx* ctx, int precision) {
-    if (!ctx || (precision != PEARL_PRECISION_FP64 && precision != PEARL_PRECISION_MIXED))
+    if (!ctx) return PEARL_ERR_INVALID_ARGUMENT;
+    if (precision < PEARL_PRECISION_FP64 || precision > PEARL_PRECISION_MIXED_SOLVE)
         return fail(ctx, PEARL_ERR_INVALID_ARGUMENT, "invalid precision");
-    ctx->P.mixed = precision == PEARL_PRECISION_MIXED;
+    const bool solve32 = precision == PEARL_PRECISION_MIXED || precision == PEARL_PRECISION_MIXED_SOLVE;
+    if (solve32 && !ctx->slab32) {
+        // FP32 planes of the inner solve: wE wN chi diag r z p0 p1 Ap
+        PG_CUDA(ctx, cudaSetDevice(ctx->device));
+        const size_t pe = plane_elems(ctx);
+        PG_CUDA(ctx, cudaMalloc(&ctx->slab32, 9 * pe * sizeof(float)));
+        PG_CUDA(ctx, cudaMemset(ctx->slab32, 0, 9 * pe * sizeof(float)));
+        float* q = ctx->slab32;
+        float** planes[9] = {&ctx->B.wE32, &ctx->B.wN32, &ctx->B.chi32, &ctx->B.diag32, &ctx->B.r32,
+                             &ctx->B.z32,  &ctx->B.p32[0], &ctx->B.p32[1], &ctx->B.Ap32};
+        for (float** pl : planes) {
+            *pl = q;
+            q += pe;
+        }
+    }
+    ctx->P.mixed = precision == PEARL_PRECISION_MIXED || precision == PEARL_PRECISION_MIXED_PROPOSE;
+    ctx->P.mixed_cg = solve32 ? 1 : 0;
+    // an FP32 round stops once its residual has fallen by this factor
+    // (PEARL_GPU_INNER_RTOL overrides)
+    ctx->P.inner_rtol = 1e-6;
+    if (const char* e = std::getenv("PEARL_GPU_INNER_RTOL")) ctx->P.inner_rtol = std::atof(e);
     return PEARL_OK;
 }
 

@@ -47,6 +47,12 @@ struct DevParams {
     // m_pa[b] + delta*(m_pb[b] + delta*m_pc[b]), so FP32 never subtracts two
     // large free energies.
     int mixed;
+    // Mixed precision of the implicit solve: FP32 inner Jacobi-PCG rounds on the
+    // correction A d = r, accumulated into the FP64 unknown, each closed by an
+    // FP64 residual of that unknown; an inner round stops once its residual has
+    // fallen by inner_rtol (or to half the tolerance).  Needs the FP32 planes.
+    int mixed_cg;
+    double inner_rtol;
     float m_obs, m_tr, m_kx, m_ky, m_rVm;  // obs, tr, 2 eps sigma / dx^2, / dy^2, 1/Vm
     float m_pa[2], m_pb[2], m_pc[2];
     float m_tau[3], m_tau_min;
@@ -98,6 +104,18 @@ struct DevBufs {
     double* wN;    // north-face weight .5*(K+K_north)/dy^2, zero at the top wall
     double* part;  // [2][grid][kMaxRed] block partials
     struct Ctl* ctl;
+    // FP32 planes of the mixed-precision solve (null until a context is put in a
+    // mixed-solve precision): the solve's face weights, susceptibility and
+    // Jacobi diagonal, and the inner CG's residual, preconditioned residual,
+    // search direction (double-buffered) and A p.
+    float* wE32;
+    float* wN32;
+    float* chi32;
+    float* diag32;
+    float* r32;
+    float* z32;
+    float* p32[2];
+    float* Ap32;
 };
 
 // Device-resident control block: barrier words, the State scalars and the
@@ -123,8 +141,11 @@ struct Ctl {
 
 enum PhaseTag : int {
     kTagPropose = 0, kTagSetup, kTagApply, kTagUpdate, kTagTrueRes, kTagReset, kTagFinal, kTagEnergy,
-    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagSmooth, kTagInit, kTagAdjoint, kTagCount
+    kTagFinalPhaseOnly, kTagMix, kTagShift, kTagSnapshot, kTagSmooth, kTagInit, kTagAdjoint,
+    kTagApply32, kTagCount
 };
+// The FP32 inner update and residual passes of the mixed solve are clocked as
+// kTagUpdate and kTagTrueRes; only the FP32 apply has a tag of its own.
 
 // ---------------------------------------------------------------- thermodynamics
 // Parabola::psi (pearl_serial.cpp:86-89)

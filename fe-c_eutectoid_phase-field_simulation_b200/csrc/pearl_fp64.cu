@@ -762,23 +762,39 @@ __device__ bool phase_setup(const Dom& a, Red& red, int cur, double dt, double& 
         S2 u = stencil2(src, 1, c.v1);
         u.c0 -= P.mu_ref; u.c1 -= P.mu_ref; u.w0 -= P.mu_ref; u.e0 -= P.mu_ref;
         u.w1 -= P.mu_ref; u.e1 -= P.mu_ref; u.s0 -= P.mu_ref; u.n1 -= P.mu_ref;
+        // the cell's set-up values; the mixed solve keeps the residual and the
+        // Jacobi step in FP32 (FP32 copies of the solve's coefficients too) and
+        // sums <r,z> of those, <r,r> of the FP64 residual
+        const auto store = [&](size_t i, double chi, const Faces& f, double u0, double rhs, double r, double diag) {
+            B.wE[i] = f.w1;
+            B.wN[i] = f.w3;
+            B.x[i] = u0;
+            if (P.mixed_cg) {
+                const float r32 = (float)r, d32 = (float)diag, z32 = __fdiv_rn(r32, d32);
+                B.wE32[i] = (float)f.w1;
+                B.wN32[i] = (float)f.w3;
+                B.chi32[i] = (float)chi;
+                B.diag32[i] = d32;
+                B.r32[i] = r32;
+                B.z32[i] = z32;
+                s1 += (double)r32 * (double)z32;
+            } else {
+                const double z = r / diag;
+                B.r[i] = r;
+                B.z[i] = z;
+                B.diag[i] = diag;
+                s1 += r * z;
+            }
+            s0 += rhs * rhs;
+            s2 += r * r;
+        };
         {
             const double chi = src.v(2, 0, kC), ic = src.v(3, 0, kC), cold = src.v(4, 0, kC);
             const Faces f = faces0(P, K, c);
             const double Au = apply0(chi, dt, f, u);
             const double diag = chi + dt * (f.w0 + f.w1 + f.w2 + f.w3);
             const double rhs = cold - ic;
-            const double r = rhs - Au;
-            const double z = r / diag;
-            B.wE[c.i0] = f.w1;
-            B.wN[c.i0] = f.w3;
-            B.x[c.i0] = u.c0;
-            B.r[c.i0] = r;
-            B.z[c.i0] = z;
-            B.diag[c.i0] = diag;
-            s0 += rhs * rhs;
-            s1 += r * z;
-            s2 += r * r;
+            store(c.i0, chi, f, u.c0, rhs, rhs - Au, diag);
         }
         if (c.v1) {
             const double chi = src.v(2, 1, kC), ic = src.v(3, 1, kC), cold = src.v(4, 1, kC);
@@ -786,17 +802,7 @@ __device__ bool phase_setup(const Dom& a, Red& red, int cur, double dt, double& 
             const double Au = apply1(chi, dt, f, u);
             const double diag = chi + dt * (f.w0 + f.w1 + f.w2 + f.w3);
             const double rhs = cold - ic;
-            const double r = rhs - Au;
-            const double z = r / diag;
-            B.wE[c.i1] = f.w1;
-            B.wN[c.i1] = f.w3;
-            B.x[c.i1] = u.c1;
-            B.r[c.i1] = r;
-            B.z[c.i1] = z;
-            B.diag[c.i1] = diag;
-            s0 += rhs * rhs;
-            s1 += r * z;
-            s2 += r * r;
+            store(c.i1, chi, f, u.c1, rhs, rhs - Au, diag);
         }
     });
     if (!ok) return false;
@@ -904,6 +910,188 @@ __device__ bool phase_reset(const Dom& a, Red& red, double& rz) {
             const double z = r / B.diag[i];
             B.z[i] = z;
             s += r * z;
+        }
+    }
+    double v[1] = {s};
+    if (!red.reduce<1>(v, kSum, kTagReset)) return false;
+    rz = v[0];
+    return true;
+}
+
+// ------------------------------------------------------------------ mixed-precision solve
+// The implicit system A u = rhs of the mixed form is solved by rounds of FP32
+// Jacobi-PCG on the correction A d = r of the current FP64 unknown x, whose
+// steps are accumulated into x in FP64; each round is closed by the FP64
+// residual of x (a plain residual pass, or the final update when the round's
+// own residual is already within the tolerance).  The operator, the
+// preconditioner and the inner vectors are FP32 planes written by SETUP.
+// These passes read their planes with plain loads (the TMA stages are sized
+// for FP64 tiles).
+
+// The tiles of this block in walk order: k-th tile of the block.
+__device__ __forceinline__ int walk_tile(const Dom& a, int k, int nb, bool reverse) {
+    return a.bid + (reverse ? nb - 1 - k : k) * a.nblk;
+}
+__device__ __forceinline__ int block_tiles(const Dom& a) {
+    return a.bid < a.P.ntiles ? (a.P.ntiles - 1 - a.bid) / a.nblk + 1 : 0;
+}
+
+struct F2 {
+    float c0, c1, w0, e0, w1, e1, s0, n1;
+};
+// Both cells' five-point stencils of an FP32 plane (as load_s2).
+__device__ __forceinline__ F2 load_f2(const float* f, const Pair& c) {
+    F2 s;
+    s.c0 = f[c.i0];
+    s.w0 = f[c.iw0];
+    s.e0 = f[c.ie0];
+    s.s0 = f[c.is0];
+    if (c.v1) {
+        s.c1 = f[c.i1];
+        s.w1 = f[c.iw1];
+        s.e1 = f[c.ie1];
+        s.n1 = f[c.in1];
+    } else {
+        s.c1 = s.c0;
+        s.w1 = s.e1 = s.n1 = 0.f;
+    }
+    return s;
+}
+
+// chi p + dt sum_f w_f (p - p_f) in FP32, with fused multiply-adds
+__device__ __forceinline__ float apply32_at(float chi, float dt, float w0, float w1, float w2, float w3, float p,
+                                            float pw, float pe, float ps, float pn) {
+    float acc = w0 * (p - pw);
+    acc = __fmaf_rn(w1, p - pe, acc);
+    acc = __fmaf_rn(w2, p - ps, acc);
+    acc = __fmaf_rn(w3, p - pn, acc);
+    return __fmaf_rn(dt, acc, chi * p);
+}
+
+// APPLY32: p = z (first) or z + beta p_old into p32[pout]; A p; <p,Ap> in FP64.
+__device__ bool phase_apply32(const Dom& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    float* pn = B.p32[pout];
+    const float* po = B.p32[pout ^ 1];
+    const float dtf = (float)dt, bf = (float)beta;
+    double s = 0;
+    const int nb = block_tiles(a);
+    for (int k = 0; k < nb; ++k) {
+        const Pair c = pair_of(P, walk_tile(a, k, nb, true));
+        if (!c.v0) continue;
+        F2 p = load_f2(B.z32, c);
+        if (!first) {
+            const F2 q = load_f2(po, c);
+            p.c0 = __fmaf_rn(bf, q.c0, p.c0);
+            p.c1 = __fmaf_rn(bf, q.c1, p.c1);
+            p.w0 = __fmaf_rn(bf, q.w0, p.w0);
+            p.e0 = __fmaf_rn(bf, q.e0, p.e0);
+            p.w1 = __fmaf_rn(bf, q.w1, p.w1);
+            p.e1 = __fmaf_rn(bf, q.e1, p.e1);
+            p.s0 = __fmaf_rn(bf, q.s0, p.s0);
+            p.n1 = __fmaf_rn(bf, q.n1, p.n1);
+        }
+        {
+            const float w0 = B.wE32[c.iw0], w1 = B.wE32[c.i0], w2 = c.y0 == 0 ? 0.f : B.wN32[c.is0],
+                        w3 = B.wN32[c.i0];
+            const float ap = apply32_at(B.chi32[c.i0], dtf, w0, w1, w2, w3, p.c0, p.w0, p.e0, p.s0, p.c1);
+            pn[c.i0] = p.c0;
+            B.Ap32[c.i0] = ap;
+            s += (double)p.c0 * (double)ap;
+        }
+        if (c.v1) {
+            const float w0 = B.wE32[c.iw1], w1 = B.wE32[c.i1], w2 = B.wN32[c.i0], w3 = B.wN32[c.i1];
+            const float ap = apply32_at(B.chi32[c.i1], dtf, w0, w1, w2, w3, p.c1, p.w1, p.e1, p.c0, p.n1);
+            pn[c.i1] = p.c1;
+            B.Ap32[c.i1] = ap;
+            s += (double)p.c1 * (double)ap;
+        }
+    }
+    double v[1] = {s};
+    if (!red.reduce<1>(v, kSum, kTagApply32)) return false;
+    pAp = v[0];
+    return true;
+}
+
+// UPDATE32: x += alpha p (FP64); r -= alpha Ap; z = r/diag; {<r,z>, <r,r>} in FP64.
+__device__ bool phase_update32(const Dom& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    const float* p = B.p32[pcur];
+    const float af = (float)alpha;
+    double s0 = 0, s1 = 0;
+    const int nb = block_tiles(a);
+    for (int k = 0; k < nb; ++k) {
+        const Pair c = pair_of(P, walk_tile(a, k, nb, false));
+        for (int j = 0; j < 2; ++j) {
+            if (!(j ? c.v1 : c.v0)) continue;
+            const size_t i = j ? c.i1 : c.i0;
+            const float pi = p[i];
+            B.x[i] = B.x[i] + alpha * (double)pi;
+            const float r = __fmaf_rn(-af, B.Ap32[i], B.r32[i]);
+            const float z = __fdiv_rn(r, B.diag32[i]);
+            B.r32[i] = r;
+            B.z32[i] = z;
+            s0 += (double)r * (double)z;
+            s1 += (double)r * (double)r;
+        }
+    }
+    double v[2] = {s0, s1};
+    if (!red.reduce<2>(v, OPS2(kSum, kSum), kTagUpdate)) return false;
+    rz = v[0];
+    rr = v[1];
+    return true;
+}
+
+// RESID32: the FP64 residual r = rhs - A x of the accumulated unknown (as the
+// final update's), handed to the next FP32 round: r32 = r, z32 = r32/diag.
+// Slots: wE, wN, x (stencils), chi, c, icpt.  Reduction {<r,r> FP64, <r32,z32>}.
+__device__ bool phase_resid32(const Dom& a, Red& red, int cur, double dt, double& rr, double& rz) {
+    const DevBufs& B = a.B;
+    double s0 = 0, s1 = 0;
+    const int maps[6] = {kMapWE, kMapWN, kMapX, kMapChi, kMapState + 5 * cur + 3, kMapIcpt};
+    const double* const planes[6] = {B.wE, B.wN, B.x, B.chi, B.c[cur], B.icpt};
+    const bool ok = sweep<6>(a, *red.pipe_ptr, maps, planes, 0x7u, true, [&](const auto& src, const Pair& c) {
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k) {
+            if (k == 1 && !c.v1) break;
+            const size_t i = k ? c.i1 : c.i0;
+            const Faces f = faces_stored(src, 0, 1, k, c);
+            const double u = src.v(2, k, kC);
+            const double r = (src.v(4, k, kC) - src.v(5, k, kC)) -
+                             apply_at(src.v(3, k, kC), dt, f, u, src.v(2, k, kW), src.v(2, k, kE), src.v(2, k, kS),
+                                      src.v(2, k, kN));
+            const float r32 = (float)r, z32 = __fdiv_rn(r32, B.diag32[i]);
+            B.r32[i] = r32;
+            B.z32[i] = z32;
+            s0 += r * r;
+            s1 += (double)r32 * (double)z32;
+        }
+    });
+    if (!ok) return false;
+    double v[2] = {s0, s1};
+    if (!red.reduce<2>(v, OPS2(kSum, kSum), kTagTrueRes)) return false;
+    rr = v[0];
+    rz = v[1];
+    return true;
+}
+
+// RESET32: after a final update whose true residual missed, that residual
+// (written by FINAL in FP64) starts the next FP32 round.  Reduction {<r32,z32>}.
+__device__ bool phase_reset32(const Dom& a, Red& red, double& rz) {
+    const DevParams& P = a.P;
+    const DevBufs& B = a.B;
+    double s = 0;
+    FOR_TILES(P) {
+        const Pair c = pair_of(P, t);
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? c.v1 : c.v0)) continue;
+            const size_t i = k ? c.i1 : c.i0;
+            const float r32 = (float)B.r[i], z32 = __fdiv_rn(r32, B.diag32[i]);
+            B.r32[i] = r32;
+            B.z32[i] = z32;
+            s += (double)r32 * (double)z32;
         }
     }
     double v[1] = {s};
@@ -1049,6 +1237,80 @@ struct DiffusionOut {
     bool bad;
 };
 
+constexpr int kMixedMaxRounds = 16;  // FP32 rounds of one mixed solve before the attempt is rejected
+
+// The mixed form's implicit diffusion: SETUP (FP64 residual, FP32 copies), FP32
+// rounds, each closed by an FP64 residual, and FINAL once a round's residual is
+// within the tolerance (pearl_serial.cpp:1010-1094 with the linear iteration
+// replaced; the convergence test, the true-residual recheck, the conservative
+// update and closure are the reference's).  o.it counts FP32 iterations.
+__device__ bool diffusion_mixed(const Dom& a, Red& red, int cur, double dt, DiffusionOut& o) {
+    const DevParams& P = a.P;
+    double rhs2, rz, rr;
+    if (!phase_setup(a, red, cur, dt, rhs2, rz, rr)) return false;
+    const double tolerance = P.cg_atol + P.cg_rtol * sqrt(rhs2);
+    int it = 0;
+    for (int round = 0; round < kMixedMaxRounds; ++round) {
+        o.it = it;
+        o.residual = sqrt(rr);
+        if (!isfinite(o.residual)) return true;
+        if (o.residual <= tolerance) {
+            // true residual and, speculatively, the update (pearl_serial.cpp:1051-1093)
+            if (!phase_final(a, red, cur, dt, o.closure, o.bad, o.mass, o.energy, rr)) return false;
+            o.residual = sqrt(rr);
+            if (o.residual <= tolerance * 1.05) {
+                o.ok = true;
+                break;
+            }
+            o.closure = 0;
+            o.bad = false;
+            o.mass = 0;
+            o.energy = 0;
+            if (!phase_reset32(a, red, rz)) return false;
+        }
+        // one FP32 round on the correction, to inner_rtol of this round's residual
+        const double target = fmax(sqrt(rr) * P.inner_rtol, 0.5 * tolerance);
+        bool first = true;
+        double beta = 0, rr32 = rr;
+        int pbuf = 0;
+        while (true) {
+            if (it >= P.cg_max) {
+                o.it = it;
+                return true;
+            }
+            const int pout = pbuf ^ 1;
+            double pAp;
+            if (!phase_apply32(a, red, dt, first, beta, pout, pAp)) return false;
+            pbuf = pout;
+            if (!(pAp > 0) || !isfinite(pAp) || !isfinite(rz)) {
+                o.it = it;
+                return true;
+            }
+            const double alpha = rz / pAp;
+            double rz_next;
+            if (!phase_update32(a, red, alpha, pbuf, rz_next, rr32)) return false;
+            ++it;
+            beta = rz_next / rz;
+            rz = rz_next;
+            first = false;
+            if (!isfinite(rr32)) {
+                o.it = it;
+                return true;
+            }
+            if (sqrt(rr32) <= target) break;
+        }
+        if (sqrt(rr32) <= tolerance) {
+            rr = rr32;  // the final update's own residual decides (next round's head)
+        } else if (!phase_resid32(a, red, cur, dt, rr, rz)) {
+            return false;
+        }
+    }
+    o.it = it;
+    if (!o.ok) return true;
+    o.ok = o.closure <= P.closure_tol;
+    return true;
+}
+
 __device__ bool diffusion(const Dom& a, Red& red, int cur, double dt, DiffusionOut& o) {
     const DevParams& P = a.P;
     o.ok = false;
@@ -1058,6 +1320,7 @@ __device__ bool diffusion(const Dom& a, Red& red, int cur, double dt, DiffusionO
     o.bad = false;
     o.mass = 0;
     o.energy = 0;
+    if (P.mixed_cg) return diffusion_mixed(a, red, cur, dt, o);
     double rhs2, rz, rr;
     if (!phase_setup(a, red, cur, dt, rhs2, rz, rr)) return false;
     const double tolerance = P.cg_atol + P.cg_rtol * sqrt(rhs2);

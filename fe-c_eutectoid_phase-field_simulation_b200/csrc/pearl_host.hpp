@@ -30,6 +30,7 @@ struct pearl_gpu_ctx {
     pearl_gpu::DevParams P{};
     pearl_gpu::DevBufs B{};
     double* slab = nullptr;
+    float* slab32 = nullptr;  // FP32 planes of the mixed solve (allocated on first use)
     pearl_gpu::Ctl* d_ctl = nullptr;
     pearl_gpu::Ctl* h_ctl = nullptr;  // pinned
     double* d_stage = nullptr;  // dense device staging of one host state (5 n doubles)

@@ -140,12 +140,14 @@ class PearlFillOp(C.Structure):
             o.p[j] = float(v)
         return o
 
-PRECISION = {"fp64": 0, "mixed": 1}
+# fp64: the reference's arithmetic; mixed: FP32 proposal + FP32 inner solve;
+# mixed_propose / mixed_solve: one of the two
+PRECISION = {"fp64": 0, "mixed": 1, "mixed_propose": 2, "mixed_solve": 3}
 # Batch group_blocks value for groups sized per instance (PEARL_BATCH_SIZED_GROUPS)
 BATCH_SIZED_GROUPS = -1
 
 PHASES = ["propose", "setup", "apply", "update", "true_residual", "reset", "final", "energy", "final_phase_only",
-          "mixture", "shift", "snapshot", "smooth", "init", "adjoint"]
+          "mixture", "shift", "snapshot", "smooth", "init", "adjoint", "apply32"]
 
 _lib = None
 
@@ -448,7 +450,8 @@ class Context:
         return st.value, ms.value
 
     def set_precision(self, precision: str) -> None:
-        """'fp64' (default, the reference's arithmetic) or 'mixed' (FP32 propose forces)."""
+        """'fp64' (default, the reference's arithmetic), 'mixed' (FP32 proposal forces and FP32
+        inner solve rounds), 'mixed_propose' or 'mixed_solve' (one of the two)."""
         self._check(self.lib.pearl_gpu_set_precision(self.h, PRECISION[precision]))
 
     def adjoint_gradient(self, nsteps: int, checkpoint_every: int, target_alpha) -> PearlAdjointReport:

@@ -137,13 +137,26 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx);
 int pearl_gpu_set_stream(pearl_gpu_ctx* ctx, void* stream);
 
 /* Arithmetic of the step.  PEARL_PRECISION_FP64 (the default) is the
- * reference's arithmetic.  PEARL_PRECISION_MIXED evaluates the propose_phi
- * forces, local tau and phase increment in FP32 (the chemical-potential
- * terms expanded about mu_reference with the offset formed in FP64); the
- * state, the projection, the implicit diffusion (PCG, residual recheck,
- * carbon update), the mass and energy reductions and every acceptance test
- * stay FP64.  No counterpart in the reference. */
-enum { PEARL_PRECISION_FP64 = 0, PEARL_PRECISION_MIXED = 1 };
+ * reference's arithmetic.  The mixed forms change two parts of it:
+ *   - FP32 proposal: the propose_phi forces, local tau and phase increment in
+ *     FP32 (the chemical-potential terms expanded about mu_reference with the
+ *     offset formed in FP64); the projection and max |dphi| stay FP64;
+ *   - FP32 inner solve: the implicit diffusion's linear system is solved by
+ *     rounds of Jacobi-PCG in FP32 on the correction of the FP64 unknown,
+ *     each round closed by its FP64 residual (iterative refinement); the
+ *     convergence test on the FP64 residual, the true-residual recheck, the
+ *     conservative carbon update and closure stay the reference's.
+ * PEARL_PRECISION_MIXED has both, PEARL_PRECISION_MIXED_PROPOSE the first
+ * only, PEARL_PRECISION_MIXED_SOLVE the second only.  The state, the mass and
+ * energy reductions and every acceptance test stay FP64 in all of them.  A
+ * form with the FP32 inner solve allocates its FP32 work planes (36 bytes per
+ * cell) on first use.  No counterpart in the reference. */
+enum {
+    PEARL_PRECISION_FP64 = 0,
+    PEARL_PRECISION_MIXED = 1,
+    PEARL_PRECISION_MIXED_PROPOSE = 2,
+    PEARL_PRECISION_MIXED_SOLVE = 3
+};
 int pearl_gpu_set_precision(pearl_gpu_ctx* ctx, int precision);
 
 /* Replace the run parameters (same grid); invalidates cached step energies. */

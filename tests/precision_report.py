@@ -7,10 +7,13 @@ helper: it runs the oracle, so it lives with the tests, not in the package).
 
 --small uses the 128x256 fixed-dt workload (10 K, 4 pairs); otherwise the large
 adaptive workload (20 K, seeded spacing and front jitter) at the given size.
-The FP64 GPU run records its accepted dt sequence; the mixed run and the
-oracle replay it, so all fields are compared at the same times.  Prints one
-JSON line: max and rms differences of phi, mu and carbon, total carbon, and
-whether each replay followed the sequence."""
+The FP64 GPU run takes N steps and sets the end time; every mixed form (and
+the oracle) runs to exactly that time, its last step clipped to it as the
+reference clips a step to an output time, so all fields are compared at the
+same physical time whatever dt sequence each form chose.  Prints one JSON
+line: per form its steps, rejections, CG iterations and seconds, and max and
+rms differences of phi, mu and carbon and the total carbon against the FP64
+GPU run and the oracle."""
 from __future__ import annotations
 
 import argparse
@@ -32,24 +35,38 @@ def _err(a, b):
     return {"max": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d)))}
 
 
-def _gpu(w, precision, steps, replay=None):
-    """Runs `steps` steps; records the accepted dt sequence, or replays `replay`."""
+def _gpu(w, precision, steps=None, stop_time=None):
+    """Runs `steps` steps, or until exactly `stop_time` (the last step is clipped
+    to it, as the reference clips a step to the next output time)."""
     import pearl_gpu
 
     with pearl_gpu.Context(w.params, w.nx, w.ny) as ctx:
         ctx.set_precision(precision)
         ctx.upload(w.phi, w.carbon, w.mu, w.scalars)
-        ctx.set_history(steps)
         t0 = time.perf_counter()
-        if replay is not None:
-            ctx.run_replay(replay)
-        else:
-            done = 0
+        done, cg = 0, 0
+        if stop_time is None:
             while done < steps:
-                done += ctx.run(min(1000, steps - done)).steps
+                r = ctx.run(min(1000, steps - done))
+                done += r.steps
+                cg += r.cg_total
+        else:
+            while ctx.scalars().time < stop_time:
+                r = ctx.run(1000, stop_time=stop_time)
+                done += r.steps
+                cg += r.cg_total
+                if r.reached_stop:
+                    break
         secs = time.perf_counter() - t0
-        hist, _ = ctx.history()
-        return ctx.download(), secs, np.array([h.accepted_dt for h in hist])
+        phi, c, mu, s = ctx.download()
+        return (phi, c, mu, s), {"time": s.time, "steps": done, "rejected": s.rejected, "cg_iterations": cg,
+                                 "seconds": secs}
+
+
+def _fields(a, b):
+    (pa, ca, ma, _), (pb, cb, mb, _) = a, b
+    return {"phi": _err(pa, pb), "mu": _err(ma, mb), "carbon": _err(ca, cb),
+            "total_carbon_rel": float(abs(ca.sum() - cb.sum()) / abs(cb.sum()))}
 
 
 def main(argv=None) -> int:
@@ -62,20 +79,22 @@ def main(argv=None) -> int:
     ap.add_argument("--small", action="store_true")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--oracle", action="store_true")
+    ap.add_argument("--forms", default="mixed,mixed_propose,mixed_solve")
     args = ap.parse_args(argv)
     if args.small:
         w = workloads.plain_small()
     else:
         w = workloads.plain_large(nx=args.nx, ny=args.ny, pairs=args.pairs or max(1, args.nx // 32))
-    (p64, c64, mu64, s64), t64, dts = _gpu(w, "fp64", args.steps)
-    # the mixed run replays the FP64 run's accepted dt sequence, so both end at the same time
-    (pmx, cmx, mumx, smx), tmx, dts_mx = _gpu(w, "mixed", args.steps, replay=dts)
-    out = {"workload": w.name, "steps": args.steps,
-           "fp64_gpu": {"time": s64.time, "rejected": s64.rejected, "seconds": t64},
-           "mixed_gpu_replay": {"time": smx.time, "rejected": smx.rejected, "seconds": tmx,
-                                "followed_dt_sequence": bool(np.array_equal(dts, dts_mx))},
-           "mixed_vs_fp64_gpu": {"phi": _err(pmx, p64), "mu": _err(mumx, mu64), "carbon": _err(cmx, c64),
-                                 "total_carbon_rel": abs(cmx.sum() - c64.sum()) / abs(c64.sum())}}
+    # the FP64 run sets the end time; every other run is clipped to exactly that time,
+    # so the fields are compared at the same physical time whatever dt each form took
+    ref, info64 = _gpu(w, "fp64", steps=args.steps)
+    end = info64["time"]
+    out = {"workload": w.name, "steps": args.steps, "end_time": end, "fp64_gpu": info64}
+    runs = {}
+    for form in [f for f in args.forms.split(",") if f]:
+        runs[form], info = _gpu(w, form, stop_time=end)
+        out[f"{form}_gpu"] = info
+        out[f"{form}_vs_fp64_gpu"] = _fields(runs[form], ref)
     if args.oracle:
         from oracle import pyoracle
 
@@ -83,11 +102,14 @@ def main(argv=None) -> int:
         po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
         so = pyoracle.scalars_from(w.scalars)
         t0 = time.perf_counter()
-        rc, why, done, _ = port.advance_n(w.params, po, co, muo, so, args.steps, forced_dt=dts)
+        # run to the end time: the step that would pass it is clipped, the one after finds no time left
+        rc, why, done, _ = port.advance_n(w.params, po, co, muo, so, 10 * args.steps + 100, stop_time=end)
         out["oracle"] = {"rc": rc, "steps": done, "time": so.time, "rejected": so.rejected,
                          "seconds": time.perf_counter() - t0}
-        out["mixed_vs_oracle"] = {"phi": _err(pmx, po), "mu": _err(mumx, muo), "carbon": _err(cmx, co)}
-        out["fp64_vs_oracle"] = {"phi": _err(p64, po), "mu": _err(mu64, muo), "carbon": _err(c64, co)}
+        orc = (po, co, muo, so)
+        out["fp64_vs_oracle"] = _fields(ref, orc)
+        for form, r in runs.items():
+            out[f"{form}_vs_oracle"] = _fields(r, orc)
     print(json.dumps(out))
     return 0
 
