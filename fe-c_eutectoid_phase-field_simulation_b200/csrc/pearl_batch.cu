@@ -245,7 +245,12 @@ int batch_launch(pearl_gpu_batch* b, const pearl_run_limits& L) {
     void* kargs[] = {&args};
     PB_CUDA(b, cudaEventRecord(b->ev0, b->stream));
     constexpr TileGeometry g = tile_geometry(8);
-    PB_CUDA(b, cudaLaunchCooperativeKernel((const void*)g8::pearl_batch_kernel, dim3(b->grid), dim3(g.threads), kargs,
+    // the mixed form's inner solve runs in a kernel of its own (all instances
+    // of a batch share one precision, pearl_gpu_batch_set_precision)
+    bool solve32 = false;
+    for (auto* c : b->inst) solve32 = solve32 || c->P.mixed_cg;
+    const void* kernel = solve32 ? (const void*)g8::pearl_batch_kernel_mixed : (const void*)g8::pearl_batch_kernel;
+    PB_CUDA(b, cudaLaunchCooperativeKernel(kernel, dim3(b->grid), dim3(g.threads), kargs,
                                            b->use_tma ? g.tma_smem_bytes : 0, b->stream));
     b->launches++;
     PB_CUDA(b, cudaEventRecord(b->ev1, b->stream));
@@ -318,15 +323,20 @@ int pearl_gpu_batch_create(int n, const pearl_params* params, const int* nx, con
     if (cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
         return bail(PEARL_ERR_CUDA);
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
-    if (tma &&
-        cudaFuncSetAttribute(g8::pearl_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tile_geometry(8).tma_smem_bytes) !=
-            cudaSuccess)
-        tma = false;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->per_sm, g8::pearl_batch_kernel, tile_geometry(8).threads,
-                                                      tma ? tile_geometry(8).tma_smem_bytes : 0) != cudaSuccess ||
-        b->per_sm < 1)
-        return bail(PEARL_ERR_CUDA);
+    const void* kernels[2] = {(const void*)g8::pearl_batch_kernel, (const void*)g8::pearl_batch_kernel_mixed};
+    for (const void* k : kernels)
+        if (tma && cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tile_geometry(8).tma_smem_bytes) != cudaSuccess)
+            tma = false;
+    b->per_sm = 1 << 30;
+    for (const void* k : kernels) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, tile_geometry(8).threads,
+                                                          tma ? tile_geometry(8).tma_smem_bytes : 0) != cudaSuccess ||
+            n < 1)
+            return bail(PEARL_ERR_CUDA);
+        b->per_sm = std::min(b->per_sm, n);
+    }
     b->tma_capable = tma;
     const int rc = batch_configure(b, group_blocks > 0 ? group_blocks : PEARL_BATCH_SIZED_GROUPS, tma, 0);
     if (rc) return bail(rc);

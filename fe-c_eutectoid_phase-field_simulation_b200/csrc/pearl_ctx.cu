@@ -73,7 +73,8 @@ void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2) {
     P.ntiles = P.ntx * P.nty;
 }
 
-const void* step_kernel(int warps) {
+const void* step_kernel(int warps, bool solve32) {
+    if (solve32) return warps == 16 ? (const void*)g16::pearl_kernel_mixed : (const void*)g8::pearl_kernel_mixed;
     return warps == 16 ? (const void*)g16::pearl_kernel : (const void*)g8::pearl_kernel;
 }
 
@@ -202,7 +203,8 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
     args.use_tma = ctx->use_tma ? 1 : 0;
     if (ctx->use_tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
     const TileGeometry g = tile_geometry(ctx->warps);
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel(step_kernel(ctx->warps), dim3(ctx->grid), dim3(g.threads), kargs,
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel(step_kernel(ctx->warps, ctx->P.mixed_cg != 0), dim3(ctx->grid),
+                                             dim3(g.threads), kargs,
                                              ctx->use_tma ? g.tma_smem_bytes : 0, ctx->stream));
     ctx->launches++;
     PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
@@ -595,14 +597,22 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     const char* tma_env = std::getenv("PEARL_GPU_TMA");
     ctx->use_tma = ctx->P.warps_x_log2 == 0 && !(tma_env && std::atoi(tma_env) == 0);
     const TileGeometry geom = tile_geometry(ctx->warps);
-    if (ctx->use_tma && cudaFuncSetAttribute(step_kernel(ctx->warps), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)geom.tma_smem_bytes) != cudaSuccess)
-        ctx->use_tma = false;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel(ctx->warps), geom.threads,
-                                                      ctx->use_tma ? geom.tma_smem_bytes : 0) != cudaSuccess ||
-        per_sm < 1)
-        return bail(PEARL_ERR_CUDA);
+    // both the FP64 kernel and the mixed-solve kernel of the block shape get the
+    // stage buffers; the grid fits the residency of both
+    for (bool solve32 : {false, true})
+        if (ctx->use_tma && cudaFuncSetAttribute(step_kernel(ctx->warps, solve32),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)geom.tma_smem_bytes) != cudaSuccess)
+            ctx->use_tma = false;
+    int per_sm = 1 << 30;
+    for (bool solve32 : {false, true}) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel(ctx->warps, solve32), geom.threads,
+                                                          ctx->use_tma ? geom.tma_smem_bytes : 0) != cudaSuccess ||
+            n < 1)
+            return bail(PEARL_ERR_CUDA);
+        per_sm = std::min(per_sm, n);
+    }
     ctx->grid = std::max(1, std::min(per_sm * sms, ctx->P.ntiles));
     // state: 2 x (3 phi + c + mu); work: K chi icpt diag x r z p0 p1 Ap  -> 20 planes
     const size_t pe = plane_elems(ctx);

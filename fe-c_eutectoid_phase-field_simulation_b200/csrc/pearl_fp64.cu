@@ -751,6 +751,9 @@ __device__ bool phase_mix(const Dom& a, Red& red, int cur, bool& mixbad) {
 
 // SETUP: apply(mu_offset) and the initial residual (pearl_serial.cpp:1036-1046).
 // Slots: K, mu (stencils), chi, icpt, c.  Reduction: {<rhs,rhs>, <r,z>, <r,r>}.
+// kSolve32: the mixed form's set-up (FP32 copies for the inner solve); the FP64
+// kernel is compiled without it.
+template <bool kSolve32>
 __device__ bool phase_setup(const Dom& a, Red& red, int cur, double dt, double& rhs2, double& rz, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
@@ -769,7 +772,7 @@ __device__ bool phase_setup(const Dom& a, Red& red, int cur, double dt, double& 
             B.wE[i] = f.w1;
             B.wN[i] = f.w3;
             B.x[i] = u0;
-            if (P.mixed_cg) {
+            if constexpr (kSolve32) {
                 const float r32 = (float)r, d32 = (float)diag, z32 = __fdiv_rn(r32, d32);
                 B.wE32[i] = (float)f.w1;
                 B.wN32[i] = (float)f.w3;
@@ -1247,7 +1250,7 @@ constexpr int kMixedMaxRounds = 16;  // FP32 rounds of one mixed solve before th
 __device__ bool diffusion_mixed(const Dom& a, Red& red, int cur, double dt, DiffusionOut& o) {
     const DevParams& P = a.P;
     double rhs2, rz, rr;
-    if (!phase_setup(a, red, cur, dt, rhs2, rz, rr)) return false;
+    if (!phase_setup<true>(a, red, cur, dt, rhs2, rz, rr)) return false;
     const double tolerance = P.cg_atol + P.cg_rtol * sqrt(rhs2);
     int it = 0;
     for (int round = 0; round < kMixedMaxRounds; ++round) {
@@ -1311,6 +1314,9 @@ __device__ bool diffusion_mixed(const Dom& a, Red& red, int cur, double dt, Diff
     return true;
 }
 
+// kSolve32: the kernel of the mixed solve (diffusion_mixed); the FP64 kernels
+// are compiled without it, so its registers do not weigh on their phases.
+template <bool kSolve32>
 __device__ bool diffusion(const Dom& a, Red& red, int cur, double dt, DiffusionOut& o) {
     const DevParams& P = a.P;
     o.ok = false;
@@ -1320,9 +1326,11 @@ __device__ bool diffusion(const Dom& a, Red& red, int cur, double dt, DiffusionO
     o.bad = false;
     o.mass = 0;
     o.energy = 0;
-    if (P.mixed_cg) return diffusion_mixed(a, red, cur, dt, o);
+    if constexpr (kSolve32) {
+        return diffusion_mixed(a, red, cur, dt, o);
+    }
     double rhs2, rz, rr;
-    if (!phase_setup(a, red, cur, dt, rhs2, rz, rr)) return false;
+    if (!phase_setup<false>(a, red, cur, dt, rhs2, rz, rr)) return false;
     const double tolerance = P.cg_atol + P.cg_rtol * sqrt(rhs2);
     bool first = true;
     double beta = 0;
@@ -1375,6 +1383,7 @@ struct StepState {
     double e0, mass0;
 };
 
+template <bool kSolve32>
 __device__ bool advance(const Dom& a, Red& red, StepState& st, double stop_time, pearl_step_info& info) {
     const DevParams& P = a.P;
     double dt = st.S.dt;
@@ -1421,7 +1430,7 @@ __device__ bool advance(const Dom& a, Red& red, StepState& st, double stop_time,
                 if (!phase_final_phase_only(a, red, st.cur, bad, e1)) return false;
             } else {
                 DiffusionOut d;
-                if (!diffusion(a, red, st.cur, dt, d)) return false;
+                if (!diffusion<kSolve32>(a, red, st.cur, dt, d)) return false;
                 good = d.ok;
                 out.cg_iterations = d.it;
                 out.linear_residual = d.residual;
@@ -1876,7 +1885,10 @@ __device__ void record_tape(const Dom& a, int cur, double* slot) {
         for (int f = 0; f < 6; ++f) slot[f * pe + i] = src[f][i];
 }
 
-__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __grid_constant__ KArgs args) {
+// The persistent step kernel's body; kSolve32 selects the mixed form's inner
+// solve (pearl_kernel_mixed), every other part is the same code.
+template <bool kSolve32>
+__device__ __forceinline__ void step_body(const KArgs& args) {
     const Dom a{args.P, args.B, args.maps, args.use_tma, (int)blockIdx.x, (int)gridDim.x, args.B.ctl, args.B.part,
                 args.shift_trigger, args.shift_target, args.shift_c_gamma, args.smooth_max_steps,
                 args.smooth_min_steps, args.smooth_energy_rtol, args.smooth_max_phase_change};
@@ -1911,7 +1923,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __gri
             }
             pearl_step_info info;
             if (args.forced_dt) st.S.dt = args.forced_dt[steps];
-            if (!advance(a, red, st, args.L.stop_time, info)) break;
+            if (!advance<kSolve32>(a, red, st, args.L.stop_time, info)) break;
             if (args.dt_log && leader) args.dt_log[steps] = info.accepted_dt;
             if (args.hist && leader) args.hist[(args.hist_next + steps) % args.hist_cap] = info;
             if (args.tape) record_tape(a, st.cur, args.tape + args.tape_slot * steps);
@@ -1960,7 +1972,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __gri
     }
     if (args.mode == kModeDiffusion) {
         DiffusionOut d;
-        if (!diffusion(a, red, st.cur, args.dt, d)) return;
+        if (!diffusion<kSolve32>(a, red, st.cur, args.dt, d)) return;
         if (leader) {
             ctl->iout[0] = d.ok;
             ctl->iout[1] = d.it;
@@ -2047,6 +2059,13 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __gri
     }
 }
 
+__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __grid_constant__ KArgs args) {
+    step_body<false>(args);
+}
+__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel_mixed(const __grid_constant__ KArgs args) {
+    step_body<true>(args);
+}
+
 // ------------------------------------------------------------------ batched instances
 // A batch advances many independent instances (own grid size, parameters,
 // dt, retries and CG count) in one cooperative launch.  The grid is split
@@ -2054,7 +2073,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_kernel(const __gri
 // group runs the same `advance` device code on its own list of instances, one
 // after another, with barriers and reductions local to the group.
 
-__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
+template <bool kSolve32>
+__device__ __forceinline__ void batch_body(const BatchArgs& args) {
     const int g = args.block_group[blockIdx.x];
     const int b0 = args.group_block0[g], nblk = args.group_block0[g + 1] - b0, bid = (int)blockIdx.x - b0;
     __shared__ PhaseClock clk;
@@ -2100,7 +2120,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_batch_kernel(const
                 break;
             }
             pearl_step_info info;
-            if (!advance(a, red, st, args.L.stop_time, info)) {
+            if (!advance<kSolve32>(a, red, st, args.L.stop_time, info)) {
                 failed = true;
                 break;
             }
@@ -2136,6 +2156,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_batch_kernel(const
         }
         red.flush();
     }
+}
+
+__global__ void __launch_bounds__(kThreads, kMinBlocks) pearl_batch_kernel(const __grid_constant__ BatchArgs args) {
+    batch_body<false>(args);
+}
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+    pearl_batch_kernel_mixed(const __grid_constant__ BatchArgs args) {
+    batch_body<true>(args);
 }
 
 // Self-test of the exact constant-divisor division: counts elements where

@@ -57,8 +57,9 @@ bool valid_params(const pearl_params* p);
 double host_psi(const pearl_params* p, int a, double mu);
 // Tile of (32 << wx) x (2 warps >> wx) cells: 2^wx warps side by side in x.
 void set_tile_shape(pearl_gpu_ctx* ctx, int wx_log2);
-// The persistent step kernel of a block shape.
-const void* step_kernel(int warps);
+// The persistent step kernel of a block shape; solve32: the kernel with the
+// mixed form's FP32 inner solve.
+const void* step_kernel(int warps, bool solve32 = false);
 // Gives the context the kernels of another block shape (tile counts and TMA
 // boxes follow); its own launch grid is kept.
 void set_geometry(pearl_gpu_ctx* ctx, int warps);

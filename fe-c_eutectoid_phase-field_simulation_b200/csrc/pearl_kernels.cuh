@@ -101,7 +101,11 @@ struct AdjArgs {
 #define PEARL_DECLARE_KERNELS(WARPS, MIN_BLOCKS)                                                                \
     __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS) pearl_kernel(const __grid_constant__ KArgs args); \
     __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS)                                                 \
+        pearl_kernel_mixed(const __grid_constant__ KArgs args);                                               \
+    __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS)                                                 \
         pearl_batch_kernel(const __grid_constant__ BatchArgs args);                                           \
+    __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS)                                                 \
+        pearl_batch_kernel_mixed(const __grid_constant__ BatchArgs args);                                     \
     __global__ void __launch_bounds__(32 * (WARPS), MIN_BLOCKS)                                                 \
         pearl_adjoint_kernel(const __grid_constant__ AdjArgs args);                                           \
     __global__ void division_selftest_kernel(const double* a, const double* b, const double* rb, long long n,  \

@@ -80,6 +80,9 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--oracle", action="store_true")
     ap.add_argument("--forms", default="mixed,mixed_propose,mixed_solve")
+    ap.add_argument("--reference-golden", action="store_true",
+                    help="--small --steps 2000|20000: also compare with the reference's own run at that step "
+                         "(tests/golden/horizon_fields.npz), which ends at the FP64 run's time")
     args = ap.parse_args(argv)
     if args.small:
         w = workloads.plain_small()
@@ -110,6 +113,15 @@ def main(argv=None) -> int:
         out["fp64_vs_oracle"] = _fields(ref, orc)
         for form, r in runs.items():
             out[f"{form}_vs_oracle"] = _fields(r, orc)
+    if args.reference_golden:
+        ref_f = np.load(ROOT / "tests" / "golden" / "horizon_fields.npz")
+        k = f"s{args.steps}"
+        assert args.small and f"{k}/phi" in ref_f.files, "the golden holds the small workload at 2000 and 20000 steps"
+        assert float(ref_f[f"{k}/scalars"][0]) == end, "the reference's run ends at another time"
+        golden = (ref_f[f"{k}/phi"], ref_f[f"{k}/carbon"], ref_f[f"{k}/mu"], None)
+        out["fp64_vs_reference"] = _fields(ref, golden)
+        for form, r in runs.items():
+            out[f"{form}_vs_reference"] = _fields(r, golden)
     print(json.dumps(out))
     return 0
 
