@@ -83,7 +83,7 @@ def parse_args(argv=None):
                          "inner-solve rounds with FP64 refinement; mixed_propose / mixed_solve: one of the two")
     ap.add_argument("--probe", choices=["propose", "diffusion", "fp64-peak"], default=None,
                     help="profiling aid instead of the bench line: launch one phase of the hot path on its own "
-                         "(propose: propose_phi + mixture; diffusion: one proposal, then the implicit solve) "
+                         "(propose: propose_phi + mixture; diffusion: one proposal, then the FP64 implicit solve) "
                          "--steps times on the --nx x --ny large workload, or measure the FP64 peak")
     ap.add_argument("--instances", type=int, default=256, help="sweep: number of instances")
     ap.add_argument("--group-blocks", type=int, default=0,

@@ -203,7 +203,9 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
     args.use_tma = ctx->use_tma ? 1 : 0;
     if (ctx->use_tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
     const TileGeometry g = tile_geometry(ctx->warps);
-    PG_CUDA(ctx, cudaLaunchCooperativeKernel(step_kernel(ctx->warps, ctx->P.mixed_cg != 0), dim3(ctx->grid),
+    // the mixed-solve kernel holds only the run mode
+    const bool solve32 = ctx->P.mixed_cg != 0 && args.mode == kModeRun;
+    PG_CUDA(ctx, cudaLaunchCooperativeKernel(step_kernel(ctx->warps, solve32), dim3(ctx->grid),
                                              dim3(g.threads), kargs,
                                              ctx->use_tma ? g.tma_smem_bytes : 0, ctx->stream));
     ctx->launches++;

@@ -295,22 +295,6 @@ __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// Arrive on a barrier; returns the token of the phase arrived on.
-__device__ __forceinline__ uint64_t mbar_arrive(uint64_t* bar) {
-    uint64_t state;
-    asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(smem_u32(bar)) : "memory");
-    return state;
-}
-// True once the phase identified by `state` (a token of mbar_arrive) has completed.
-__device__ __forceinline__ bool mbar_try_wait_token(uint64_t* bar, uint64_t state) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "l"(state)
-        : "memory");
-    return ok != 0;
-}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(

@@ -363,48 +363,33 @@ __device__ __forceinline__ Faces faces_stored(const Src& src, int se, int sn, in
 
 // ------------------------------------------------------------------ TMA pipeline
 // Stage s of the pipeline has a "full" barrier (one arrival with the expected
-// bytes, completed by the copies).  With 16-warp blocks (one per SM, so a block
-// barrier would idle the whole SM) it also has an "empty" barrier (one arrival
-// per warp when the warp is done with the stage's tile) and a counter that
-// elects the last warp to finish a tile: that warp refills the stage, and no
-// block-wide barrier separates tiles, so a warp may run ahead into tiles
-// already staged (2048x4096: 1.653 vs 1.661 ms/step).  With 8-warp blocks,
-// two per SM, the block barrier that ends each tile frees the stage instead
-// (the per-warp form measured no faster there).
-constexpr int kWarps = kThreads / 32;
-constexpr bool kWarpPipeline = kWarps >= 16;
-constexpr size_t kPipeHeaderBytes = 128;  // full[4], empty[4] mbarriers, counters[4]
-static_assert(2 * kMaxStages * sizeof(uint64_t) + kMaxStages * sizeof(unsigned) <= kPipeHeaderBytes,
-              "pipeline header");
+// bytes, completed by the copies); the block barrier that ends each tile frees
+// the stage, and thread 0 then refills it with the tile S-1 ahead.  (Freeing
+// stages warp by warp through "empty" barriers, so that a warp could run ahead
+// into staged tiles, measured 1.686 against 1.683 ms/step with 512-thread
+// blocks on 2048x4096, five runs each on one GPU, and was dropped.)
+constexpr size_t kPipeHeaderBytes = 128;  // full[4] mbarriers
+static_assert(kMaxStages * sizeof(uint64_t) <= kPipeHeaderBytes, "pipeline header");
 struct Pipe {
     uint64_t* bar;     // kMaxStages "full" mbarriers in shared memory
-    uint64_t* empty;   // kMaxStages "empty" mbarriers (kWarps arrivals per phase)
-    unsigned* cnt;     // kMaxStages warp counters (kWarps per tile, never reset)
     double* stage;     // stage buffers (kPipeDoubles)
     uint32_t parity;   // bit s: next completion phase expected on barrier s
 };
 
 __device__ __forceinline__ Pipe make_pipe(unsigned char* dsmem) {
-    uint64_t* b = reinterpret_cast<uint64_t*>(dsmem);
-    return Pipe{b, b + kMaxStages, reinterpret_cast<unsigned*>(b + 2 * kMaxStages),
-                reinterpret_cast<double*>(dsmem + kPipeHeaderBytes), 0u};
+    return Pipe{reinterpret_cast<uint64_t*>(dsmem), reinterpret_cast<double*>(dsmem + kPipeHeaderBytes), 0u};
 }
 // Thread 0 initialises the barriers; the caller synchronises the block after.
 __device__ __forceinline__ void init_pipe(const Pipe& pp) {
-    for (int s = 0; s < kMaxStages; ++s) {
-        mbar_init(&pp.bar[s], 1);
-        mbar_init(&pp.empty[s], kWarps);
-        pp.cnt[s] = 0;
-    }
+    for (int s = 0; s < kMaxStages; ++s) mbar_init(&pp.bar[s], 1);
     mbar_fence_init();
 }
 
 // Bounded waits on a pipeline barrier.  A wait gives up after limit_ns, or
-// early once another warp of the block group has recorded a device-wait
-// timeout in *abort_status (a tile that warp left unfinished is never
-// refilled, so waiting out the full limit again would only double the time the
-// error path takes).  Drains of in-flight copies pass no abort_status: they
-// must wait for the copies themselves.
+// early once another block of the group has recorded a device-wait timeout in
+// *abort_status (the launch is failing, so waiting out the full limit again
+// would only lengthen the error path).  Drains of in-flight copies pass no
+// abort_status: they must wait for the copies themselves.
 __device__ __forceinline__ bool wait_aborted(const int* abort_status) {
     return abort_status && *(const volatile int*)abort_status == (int)PEARL_ERR_DEVICE_WAIT;
 }
@@ -418,17 +403,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
         if ((it & 63u) == 0 && (globaltimer_ns() - t0 > limit_ns || wait_aborted(abort_status))) return false;
     }
 }
-__device__ __forceinline__ bool mbar_wait_token_bounded(uint64_t* bar, uint64_t state,
-                                                        const int* abort_status = nullptr) {
-    if (mbar_try_wait_token(bar, state)) return true;
-    const unsigned long long t0 = globaltimer_ns();
-    for (unsigned it = 1;; ++it) {
-        if (mbar_try_wait_token(bar, state)) return true;
-        if ((it & 63u) == 0 && (globaltimer_ns() - t0 > kBarrierTimeoutNs || wait_aborted(abort_status)))
-            return false;
-    }
-}
-
 // Sweep the block's tiles, calling body(src, pair) for every tile whose first
 // cell is inside the domain.  With TMA, field slot k of tile t is staged from
 // tensor map maps[k]; slots whose bit is set in `stencil` also get the
@@ -481,18 +455,16 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
     // staged in it, or read only at the cells that the reading block itself
     // writes, after reading them)
     if (lane == 0) fence_proxy_async();
-    // S tiles ahead when warps free stages one by one, S-1 when the block barrier does
+    // S-1 tiles ahead: the stage of tile k+S-1 is the one freed by the barrier ending tile k-1
     if (threadIdx.x == 0)
-        for (int k = 0; k < (kWarpPipeline ? S : S - 1) && k < nb; ++k) issue(k);
+        for (int k = 0; k < S - 1 && k < nb; ++k) issue(k);
     for (int k = 0; k < nb; ++k) {
         const int s = k % S;
-        if (!kWarpPipeline && threadIdx.x == 0 && k + S - 1 < nb) issue(k + S - 1);
+        if (threadIdx.x == 0 && k + S - 1 < nb) issue(k + S - 1);
         if (!mbar_wait_bounded(&pp.bar[s], (pp.parity >> s) & 1u, kBarrierTimeoutNs, &a.bar->status)) {
             atomicCAS(&a.bar->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
             // drain the copies that may still be in flight, this tile's included
-            // when the wait was cut short by another warp's timeout (a tile is
-            // staged only once its stage's previous tile was finished by every
-            // warp), bounded
+            // when the wait was cut short by another block's timeout, bounded
             for (int j = k; j < nb && j < k + S; ++j)
                 mbar_wait_bounded(&pp.bar[j % S], (pp.parity >> (j % S)) & 1u, kBarrierTimeoutNs / 16);
             return false;
@@ -521,24 +493,7 @@ __device__ bool sweep(const Dom& a, Pipe& pp, const int (&maps)[NF], const doubl
                                         : SmemSrc<NF>{st, lane + 2, 2 * warp + 1, c.y0 > 0, c.v1, c.y0 + 2 < P.ny, kBoxW};
             body(src, c);
         }
-        if (!kWarpPipeline) {
-            __syncthreads();  // every warp is done with stage s: it is refilled next iteration
-            continue;
-        }
-        // done with the stage: every warp arrives, then counts; the warp whose count
-        // completes the tile (all warps arrived before counting, so its wait on the
-        // empty barrier returns at once) stages tile k+S in it
-        __syncwarp();
-        if (lane == 0) {
-            const uint64_t token = mbar_arrive(&pp.empty[s]);
-            const unsigned before = atomicAdd(&pp.cnt[s], 1u);
-            if (before % kWarps == kWarps - 1 && k + S < nb) {
-                if (!mbar_wait_token_bounded(&pp.empty[s], token, &a.bar->status))
-                    atomicCAS(&a.bar->status, 0, (int)PEARL_ERR_DEVICE_WAIT);
-                else
-                    issue(k + S);
-            }
-        }
+        __syncthreads();  // every warp is done with stage s: it is refilled next iteration
     }
     return true;
 }
@@ -972,18 +927,24 @@ __device__ __forceinline__ float apply32_at(float chi, float dt, float w0, float
 }
 
 // APPLY32: p = z (first) or z + beta p_old into p32[pout]; A p; <p,Ap> in FP64.
+// The planes are distinct, so every load of a tile is issued before its stores.
 __device__ bool phase_apply32(const Dom& a, Red& red, double dt, bool first, double beta, int pout, double& pAp) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    float* pn = B.p32[pout];
-    const float* po = B.p32[pout ^ 1];
+    float* __restrict__ pn = B.p32[pout];
+    float* __restrict__ apo = B.Ap32;
+    const float* __restrict__ po = B.p32[pout ^ 1];
+    const float* __restrict__ z32 = B.z32;
+    const float* __restrict__ wE = B.wE32;
+    const float* __restrict__ wN = B.wN32;
+    const float* __restrict__ chi = B.chi32;
     const float dtf = (float)dt, bf = (float)beta;
     double s = 0;
     const int nb = block_tiles(a);
     for (int k = 0; k < nb; ++k) {
         const Pair c = pair_of(P, walk_tile(a, k, nb, true));
         if (!c.v0) continue;
-        F2 p = load_f2(B.z32, c);
+        F2 p = load_f2(z32, c);
         if (!first) {
             const F2 q = load_f2(po, c);
             p.c0 = __fmaf_rn(bf, q.c0, p.c0);
@@ -995,20 +956,23 @@ __device__ bool phase_apply32(const Dom& a, Red& red, double dt, bool first, dou
             p.s0 = __fmaf_rn(bf, q.s0, p.s0);
             p.n1 = __fmaf_rn(bf, q.n1, p.n1);
         }
-        {
-            const float w0 = B.wE32[c.iw0], w1 = B.wE32[c.i0], w2 = c.y0 == 0 ? 0.f : B.wN32[c.is0],
-                        w3 = B.wN32[c.i0];
-            const float ap = apply32_at(B.chi32[c.i0], dtf, w0, w1, w2, w3, p.c0, p.w0, p.e0, p.s0, p.c1);
-            pn[c.i0] = p.c0;
-            B.Ap32[c.i0] = ap;
-            s += (double)p.c0 * (double)ap;
-        }
+        const float a0 = wE[c.iw0], a1 = wE[c.i0], a2 = c.y0 == 0 ? 0.f : wN[c.is0], a3 = wN[c.i0], x0 = chi[c.i0];
+        float b0 = 0.f, b1 = 0.f, b3 = 0.f, x1 = 0.f;
         if (c.v1) {
-            const float w0 = B.wE32[c.iw1], w1 = B.wE32[c.i1], w2 = B.wN32[c.i0], w3 = B.wN32[c.i1];
-            const float ap = apply32_at(B.chi32[c.i1], dtf, w0, w1, w2, w3, p.c1, p.w1, p.e1, p.c0, p.n1);
+            b0 = wE[c.iw1];
+            b1 = wE[c.i1];
+            b3 = wN[c.i1];
+            x1 = chi[c.i1];
+        }
+        const float ap0 = apply32_at(x0, dtf, a0, a1, a2, a3, p.c0, p.w0, p.e0, p.s0, p.c1);
+        pn[c.i0] = p.c0;
+        apo[c.i0] = ap0;
+        s += (double)p.c0 * (double)ap0;
+        if (c.v1) {
+            const float ap1 = apply32_at(x1, dtf, b0, b1, a3, b3, p.c1, p.w1, p.e1, p.c0, p.n1);
             pn[c.i1] = p.c1;
-            B.Ap32[c.i1] = ap;
-            s += (double)p.c1 * (double)ap;
+            apo[c.i1] = ap1;
+            s += (double)p.c1 * (double)ap1;
         }
     }
     double v[1] = {s};
@@ -1018,24 +982,46 @@ __device__ bool phase_apply32(const Dom& a, Red& red, double dt, bool first, dou
 }
 
 // UPDATE32: x += alpha p (FP64); r -= alpha Ap; z = r/diag; {<r,z>, <r,r>} in FP64.
+// Both cells' loads are issued before any store.
 __device__ bool phase_update32(const Dom& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
-    const float* p = B.p32[pcur];
+    const float* __restrict__ p = B.p32[pcur];
+    const float* __restrict__ ap = B.Ap32;
+    const float* __restrict__ dg = B.diag32;
+    float* __restrict__ r32 = B.r32;
+    float* __restrict__ z32 = B.z32;
+    double* __restrict__ x = B.x;
     const float af = (float)alpha;
     double s0 = 0, s1 = 0;
     const int nb = block_tiles(a);
     for (int k = 0; k < nb; ++k) {
         const Pair c = pair_of(P, walk_tile(a, k, nb, false));
-        for (int j = 0; j < 2; ++j) {
-            if (!(j ? c.v1 : c.v0)) continue;
-            const size_t i = j ? c.i1 : c.i0;
-            const float pi = p[i];
-            B.x[i] = B.x[i] + alpha * (double)pi;
-            const float r = __fmaf_rn(-af, B.Ap32[i], B.r32[i]);
-            const float z = __fdiv_rn(r, B.diag32[i]);
-            B.r32[i] = r;
-            B.z32[i] = z;
+        if (!c.v0) continue;
+        const float p0 = p[c.i0], ap0 = ap[c.i0], r0 = r32[c.i0], d0 = dg[c.i0];
+        const double x0 = x[c.i0];
+        float p1 = 0.f, ap1 = 0.f, r1 = 0.f, d1 = 1.f;
+        double x1 = 0;
+        if (c.v1) {
+            p1 = p[c.i1];
+            ap1 = ap[c.i1];
+            r1 = r32[c.i1];
+            d1 = dg[c.i1];
+            x1 = x[c.i1];
+        }
+        {
+            const float r = __fmaf_rn(-af, ap0, r0), z = __fdiv_rn(r, d0);
+            x[c.i0] = x0 + alpha * (double)p0;
+            r32[c.i0] = r;
+            z32[c.i0] = z;
+            s0 += (double)r * (double)z;
+            s1 += (double)r * (double)r;
+        }
+        if (c.v1) {
+            const float r = __fmaf_rn(-af, ap1, r1), z = __fdiv_rn(r, d1);
+            x[c.i1] = x1 + alpha * (double)p1;
+            r32[c.i1] = r;
+            z32[c.i1] = z;
             s0 += (double)r * (double)z;
             s1 += (double)r * (double)r;
         }
@@ -1243,17 +1229,23 @@ struct DiffusionOut {
 constexpr int kMixedMaxRounds = 16;  // FP32 rounds of one mixed solve before the attempt is rejected
 
 // The mixed form's implicit diffusion: SETUP (FP64 residual, FP32 copies), FP32
-// rounds, each closed by an FP64 residual, and FINAL once a round's residual is
-// within the tolerance (pearl_serial.cpp:1010-1094 with the linear iteration
+// rounds, each closed by an FP64 residual, and FINAL once a residual is within
+// the tolerance (pearl_serial.cpp:1010-1094 with the linear iteration
 // replaced; the convergence test, the true-residual recheck, the conservative
-// update and closure are the reference's).  o.it counts FP32 iterations.
+// update and closure are the reference's).  One pass per loop turn, as in the
+// FP64 solve: rr holds the residual estimate of the last pass (FP64 after
+// SETUP, RESID32 and FINAL, FP32 after an inner update); o.it counts FP32
+// iterations.
 __device__ bool diffusion_mixed(const Dom& a, Red& red, int cur, double dt, DiffusionOut& o) {
     const DevParams& P = a.P;
     double rhs2, rz, rr;
     if (!phase_setup<true>(a, red, cur, dt, rhs2, rz, rr)) return false;
     const double tolerance = P.cg_atol + P.cg_rtol * sqrt(rhs2);
-    int it = 0;
-    for (int round = 0; round < kMixedMaxRounds; ++round) {
+    double target = fmax(sqrt(rr) * P.inner_rtol, 0.5 * tolerance);  // this round's stop
+    bool first = true;
+    double beta = 0;
+    int pbuf = 0, rounds = 1, it = 0;
+    while (true) {
         o.it = it;
         o.residual = sqrt(rr);
         if (!isfinite(o.residual)) return true;
@@ -1270,46 +1262,29 @@ __device__ bool diffusion_mixed(const Dom& a, Red& red, int cur, double dt, Diff
             o.mass = 0;
             o.energy = 0;
             if (!phase_reset32(a, red, rz)) return false;
-        }
-        // one FP32 round on the correction, to inner_rtol of this round's residual
-        const double target = fmax(sqrt(rr) * P.inner_rtol, 0.5 * tolerance);
-        bool first = true;
-        double beta = 0, rr32 = rr;
-        int pbuf = 0;
-        while (true) {
-            if (it >= P.cg_max) {
-                o.it = it;
-                return true;
-            }
+        } else if (!first && o.residual <= target) {
+            // the round reached its stop: the FP64 residual of the accumulated unknown
+            if (!phase_resid32(a, red, cur, dt, rr, rz)) return false;
+        } else {
+            if (it >= P.cg_max) return true;
             const int pout = pbuf ^ 1;
             double pAp;
             if (!phase_apply32(a, red, dt, first, beta, pout, pAp)) return false;
             pbuf = pout;
-            if (!(pAp > 0) || !isfinite(pAp) || !isfinite(rz)) {
-                o.it = it;
-                return true;
-            }
-            const double alpha = rz / pAp;
+            if (!(pAp > 0) || !isfinite(pAp) || !isfinite(rz)) return true;
             double rz_next;
-            if (!phase_update32(a, red, alpha, pbuf, rz_next, rr32)) return false;
+            if (!phase_update32(a, red, rz / pAp, pbuf, rz_next, rr)) return false;
             ++it;
             beta = rz_next / rz;
             rz = rz_next;
             first = false;
-            if (!isfinite(rr32)) {
-                o.it = it;
-                return true;
-            }
-            if (sqrt(rr32) <= target) break;
+            continue;
         }
-        if (sqrt(rr32) <= tolerance) {
-            rr = rr32;  // the final update's own residual decides (next round's head)
-        } else if (!phase_resid32(a, red, cur, dt, rr, rz)) {
-            return false;
-        }
+        // a new round from the FP64 residual just formed
+        if (++rounds > kMixedMaxRounds) return true;
+        target = fmax(sqrt(rr) * P.inner_rtol, 0.5 * tolerance);
+        first = true;
     }
-    o.it = it;
-    if (!o.ok) return true;
     o.ok = o.closure <= P.closure_tol;
     return true;
 }
@@ -1951,6 +1926,10 @@ __device__ __forceinline__ void step_body(const KArgs& args) {
         red.flush();
         return;
     }
+    // the mixed-solve kernel runs only the run mode (the host launches every
+    // other mode, none of which solves, in the FP64 kernel; a second solving
+    // mode here would double the solve's code and its register pressure)
+    if constexpr (kSolve32) return;
     if (args.mode == kModePropose) {
         double change;
         bool mixbad, simplexbad;

@@ -253,7 +253,9 @@ int pearl_gpu_init_composition(pearl_gpu_ctx* ctx, double mu, double* total_carb
 int pearl_gpu_propose_phi(pearl_gpu_ctx* ctx, double dt, double* max_change);
 /* Uploads phase fractions into the trial buffer (the trial.phi of implicit_diffusion). */
 int pearl_gpu_upload_trial_phi(pearl_gpu_ctx* ctx, const double* phi_aos3);
-/* implicit_diffusion (pearl_serial.cpp:1010-1094) on the trial phi; writes trial carbon and mu. */
+/* implicit_diffusion (pearl_serial.cpp:1010-1094) on the trial phi; writes trial carbon and mu.
+ * Always the reference's FP64 solve, whatever the context's precision (the
+ * mixed forms' inner solve runs only inside pearl_gpu_advance / _run). */
 int pearl_gpu_implicit_diffusion(pearl_gpu_ctx* ctx, double dt, int* ok, int* iterations, double* residual,
                                  double* closure);
 int pearl_gpu_download_trial(pearl_gpu_ctx* ctx, double* phi_aos3, double* carbon, double* mu);
