@@ -197,23 +197,31 @@ class ClockSampler:
             self._nvml = None
             return
         self._stop = threading.Event()
+        first = threading.Event()
 
         def run():
             P = self._nvml
             get_reasons = getattr(P, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
                 P.nvmlDeviceGetCurrentClocksThrottleReasons
             max_mhz = float(P.nvmlDeviceGetMaxClockInfo(handle, P.NVML_CLOCK_SM))
-            while not self._stop.is_set():
+            while True:
                 try:
                     sm = float(P.nvmlDeviceGetClockInfo(handle, P.NVML_CLOCK_SM))
                     reasons = int(get_reasons(handle))
                 except Exception:  # noqa: BLE001
                     break
                 self.samples.append((sm, max_mhz, reasons))
+                first.set()
+                # one more sample after stop() is called: the end of the timed region
+                if self._stop.is_set():
+                    break
                 self._stop.wait(self.period)
+            first.set()
 
         self._thread = threading.Thread(target=run, daemon=True)
         self._thread.start()
+        # the sampler is running before the timed region starts
+        first.wait(timeout=2.0)
 
     def stop(self) -> dict | None:
         if self._thread is None:
