@@ -84,6 +84,24 @@ __device__ __forceinline__ double div_by(const DevParams& P, double a, double b,
     return special ? q0 : q;
 }
 
+// div_by for the proposal's forces (positive divisors only): the same
+// correctly rounded quotient for finite numerators and quotients, but without
+// div_by's integer tests.  A zero numerator's sign is OR-ed into the result
+// (the corrections turn -0 into +0, and a nonzero quotient already has the
+// numerator's sign); a non-finite numerator gives NaN where IEEE division
+// gives +-Inf.  Both are non-finite, and the proposal treats any non-finite
+// force alike: the cell takes the reference's non-finite branch
+// (pearl_serial.cpp:990-996), keeps its phi and reports an infinite change.
+__device__ __forceinline__ double div_force(const DevParams& P, double a, double b, double rb) {
+    if (!P.exact_div) return a / b;
+    const double q0 = a * rb;
+    double r = fma(-q0, b, a);
+    double q = fma(r, rb, q0);
+    r = fma(-q, b, a);
+    q = fma(r, rb, q);
+    return __hiloint2double(__double2hiint(q) | (__double2hiint(a) & (int)0x80000000), __double2loint(q));
+}
+
 // Device buffers: two state sets (current / trial, selected by Ctl::cur) and
 // the work vectors of the implicit solve.  Every plane is ny rows of `pitch`
 // doubles (pitch = nx rounded up to 32, so each row starts on 256 B).

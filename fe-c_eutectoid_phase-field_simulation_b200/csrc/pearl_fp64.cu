@@ -525,7 +525,7 @@ __device__ __forceinline__ Proposal propose_cell(const DevParams& P, const Src& 
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             const double dh = dtr[aa] + (b == aa ? 6.0 * q[b] * (1.0 - q[b]) : 0.0);
-            f[aa] += div_by(P, (ps[b] - psi0) * dh, P.Vm, P.r_Vm);
+            f[aa] += div_force(P, (ps[b] - psi0) * dh, P.Vm, P.r_Vm);
         }
     }
     // four faces in the reference's order: -x, +x, -y (not at y=0), +y (not at the top)
@@ -539,12 +539,12 @@ __device__ __forceinline__ Proposal propose_cell(const DevParams& P, const Src& 
         for (int aa = 0; aa < 3; ++aa)
 #pragma unroll
             for (int b = aa + 1; b < 3; ++b) {
-                const double w = div_by(P, P.two_eps_sigma * (q[aa] * n[b] - n[aa] * q[b]), d2, rd2);
+                const double w = div_force(P, P.two_eps_sigma * (q[aa] * n[b] - n[aa] * q[b]), d2, rd2);
                 f[aa] += w * n[b];
                 f[b] -= w * n[aa];
             }
     }
-    const double mean = div_by(P, f[0] + f[1] + f[2], 3.0, P.r_3);
+    const double mean = div_force(P, f[0] + f[1] + f[2], 3.0, P.r_3);
     const double scale = dt / (local_tau(P, q0, q1, q2) * P.eps);
     Proposal o;
     o.z0 = q0 - scale * (f[0] - mean);

@@ -56,6 +56,36 @@ def test_division_algorithm_exact_on_cpu():
             assert q == ref and np.signbit(q) == np.signbit(ref), (a, b)
 
 
+def _div_force(a: float, b: float, rb: float) -> float:
+    """The proposal's variant: the corrections applied to every numerator, the
+    numerator's sign bit OR-ed into the result (no tests on the operands)."""
+    q0 = a * rb
+    r = _fma(-q0, b, a)
+    q = _fma(r, rb, q0)
+    r = _fma(-q, b, a)
+    q = _fma(r, rb, q)
+    return -abs(q) if np.signbit(a) else q
+
+
+def test_force_division_exact_for_finite_quotients_on_cpu():
+    """div_force equals IEEE division, sign of zero included, for the positive
+    constant divisors and every finite numerator whose quotient is a normal
+    number (the proposal's forces are far inside that range; a non-finite force
+    takes the reference's non-finite branch whatever its value)."""
+    rng = np.random.default_rng(12)
+    for b in _divisors():
+        if b <= 0:
+            continue
+        rb = 1.0 / b
+        for a in _numerators(rng, 400, b):
+            a = float(a)
+            ref = a / b
+            if not np.isfinite(ref) or (ref != 0.0 and abs(ref) < np.finfo(float).tiny):
+                continue
+            q = _div_force(a, b, rb)
+            assert q == ref and np.signbit(q) == np.signbit(ref), (a, b)
+
+
 @pytest.mark.gpu
 def test_division_device_exact(gpu_lib):
     import pearl_gpu
