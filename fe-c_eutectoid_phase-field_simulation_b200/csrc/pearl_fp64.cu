@@ -176,6 +176,11 @@ __device__ __forceinline__ double flux_at(double dt, const Faces& f, double u, d
 struct Phi3 {
     double a, t, g;
 };
+#define DIVC(P, a, b, rb) (kForce ? div_force(P, a, b, rb) : div_by(P, a, b, rb))
+// kForce: the final update's evaluation, whose divisions skip div_by's
+// operand tests (div_force): the same value for a finite state, and a state
+// that is not finite is rejected by valid_state before its energy is looked at.
+template <bool kForce = false>
 __device__ __forceinline__ double energy_cell(const DevParams& P, const Phi3& q, const Phi3& e, const Phi3& n,
                                               bool has_n, double carbon, double chi, double icpt) {
     const double triple = 2.0 * q.a * q.t * q.g;
@@ -190,25 +195,27 @@ __device__ __forceinline__ double energy_cell(const DevParams& P, const Phi3& q,
         const double dc = carbon - icpt;
         chem += .5 * dc * dc / chi;
     }
-    double t = div_by(P, chem, P.Vm, P.r_Vm) + P.obs * (q.a * q.t + q.a * q.g + q.t * q.g) + P.tr * q.a * q.t * q.g;
-    double z = div_by(P, q.a * e.t - e.a * q.t, P.dx, P.r_dx);
+    double t = DIVC(P, chem, P.Vm, P.r_Vm) + P.obs * (q.a * q.t + q.a * q.g + q.t * q.g) + P.tr * q.a * q.t * q.g;
+    double z = DIVC(P, q.a * e.t - e.a * q.t, P.dx, P.r_dx);
     t += P.eps_sigma * z * z;
-    z = div_by(P, q.a * e.g - e.a * q.g, P.dx, P.r_dx);
+    z = DIVC(P, q.a * e.g - e.a * q.g, P.dx, P.r_dx);
     t += P.eps_sigma * z * z;
-    z = div_by(P, q.t * e.g - e.t * q.g, P.dx, P.r_dx);
+    z = DIVC(P, q.t * e.g - e.t * q.g, P.dx, P.r_dx);
     t += P.eps_sigma * z * z;
     if (has_n) {
-        z = div_by(P, q.a * n.t - n.a * q.t, P.dy, P.r_dy);
+        z = DIVC(P, q.a * n.t - n.a * q.t, P.dy, P.r_dy);
         t += P.eps_sigma * z * z;
-        z = div_by(P, q.a * n.g - n.a * q.g, P.dy, P.r_dy);
+        z = DIVC(P, q.a * n.g - n.a * q.g, P.dy, P.r_dy);
         t += P.eps_sigma * z * z;
-        z = div_by(P, q.t * n.g - n.t * q.g, P.dy, P.r_dy);
+        z = DIVC(P, q.t * n.g - n.t * q.g, P.dy, P.r_dy);
         t += P.eps_sigma * z * z;
     }
     return t;
 }
 
 // valid_state per cell (pearl_serial.cpp:1099-1114); true if the cell is bad.
+// kForce: as energy_cell (a non-finite mu fails the test before its quotient).
+template <bool kForce = false>
 __device__ __forceinline__ bool bad_cell(const DevParams& P, const Phi3& q, double carbon, double mu) {
     bool good = true;
     double sum = 0;
@@ -226,12 +233,14 @@ __device__ __forceinline__ bool bad_cell(const DevParams& P, const Phi3& q, doub
 #pragma unroll
         for (int a = 0; a < 3; ++a)
             if (qq[a] > .01) {
-                const double ca = div_by(P, mu - P.B[a], P.two_A[a], P.r_two_A[a]);
+                const double ca = DIVC(P, mu - P.B[a], P.two_A[a], P.r_two_A[a]);
                 good = good && ca >= -1e-10 && ca <= 1 + 1e-10;
             }
     }
     return !good;
 }
+
+#undef DIVC
 
 __device__ __forceinline__ Phi3 load_phi(const double* const* ph, size_t i) { return Phi3{ph[0][i], ph[1][i], ph[2][i]}; }
 
@@ -1130,9 +1139,9 @@ __device__ bool phase_final(const Dom& a, Red& red, int cur, double dt, double& 
             const Phi3 q{src.v(3, k, kC), src.v(4, k, kC), src.v(5, k, kC)};
             const Phi3 e{src.v(3, k, kE), src.v(4, k, kE), src.v(5, k, kE)};
             const Phi3 n = has_n ? Phi3{src.v(3, k, kN), src.v(4, k, kN), src.v(5, k, kN)} : Phi3{0, 0, 0};
-            if (bad_cell(P, q, cn, mun)) vbad = 1;
+            if (bad_cell<true>(P, q, cn, mun)) vbad = 1;
             vmass += cn;
-            ven += energy_cell(P, q, e, n, has_n, cn, chi, icpt);
+            ven += energy_cell<true>(P, q, e, n, has_n, cn, chi, icpt);
         }
     });
     if (!ok) return false;
