@@ -127,11 +127,13 @@ __device__ __forceinline__ S2 load_s2(const double* f, const Pair& c) {
 struct Faces {
     double w0, w1, w2, w3;
 };
+// K is finite and nonnegative here (SET-UP runs only on a trial whose mixture
+// passed its checks, pearl_serial.cpp:136), so div_force gives div_by's bits.
 __device__ __forceinline__ double face_x(const DevParams& P, double k, double kn) {
-    return div_by(P, .5 * (k + kn), P.dx2, P.r_dx2);
+    return div_force(P, .5 * (k + kn), P.dx2, P.r_dx2);
 }
 __device__ __forceinline__ double face_y(const DevParams& P, double k, double kn) {
-    return div_by(P, .5 * (k + kn), P.dy2, P.r_dy2);
+    return div_force(P, .5 * (k + kn), P.dy2, P.r_dy2);
 }
 __device__ __forceinline__ Faces faces0(const DevParams& P, const S2& K, const Pair& c) {
     Faces f;
