@@ -993,7 +993,13 @@ __device__ bool phase_apply32(const Dom& a, Red& red, double dt, bool first, dou
 }
 
 // UPDATE32: x += alpha p (FP64); r -= alpha Ap; z = r/diag; {<r,z>, <r,r>} in FP64.
-// Both cells' loads are issued before any store.
+// Pointwise, so it runs over groups of four consecutive cells of a row: one
+// 16-byte load per FP32 plane and two per FP64 plane a group (rows start on
+// 128 bytes and the pitch is a multiple of 32 cells), which keeps enough bytes
+// in flight without a staging pipeline.  Group g belongs to thread g mod
+// (blocks x threads) of the block group, a fixed assignment, so the sums are
+// deterministic; cells of the row padding (x >= nx) keep their values and add
+// nothing.
 __device__ bool phase_update32(const Dom& a, Red& red, double alpha, int pcur, double& rz, double& rr) {
     const DevParams& P = a.P;
     const DevBufs& B = a.B;
@@ -1005,37 +1011,36 @@ __device__ bool phase_update32(const Dom& a, Red& red, double alpha, int pcur, d
     double* __restrict__ x = B.x;
     const float af = (float)alpha;
     double s0 = 0, s1 = 0;
-    const int nb = block_tiles(a);
-    for (int k = 0; k < nb; ++k) {
-        const Pair c = pair_of(P, walk_tile(a, k, nb, false));
-        if (!c.v0) continue;
-        const float p0 = p[c.i0], ap0 = ap[c.i0], r0 = r32[c.i0], d0 = dg[c.i0];
-        const double x0 = x[c.i0];
-        float p1 = 0.f, ap1 = 0.f, r1 = 0.f, d1 = 1.f;
-        double x1 = 0;
-        if (c.v1) {
-            p1 = p[c.i1];
-            ap1 = ap[c.i1];
-            r1 = r32[c.i1];
-            d1 = dg[c.i1];
-            x1 = x[c.i1];
-        }
-        {
-            const float r = __fmaf_rn(-af, ap0, r0), z = __fdiv_rn(r, d0);
-            x[c.i0] = x0 + alpha * (double)p0;
-            r32[c.i0] = r;
-            z32[c.i0] = z;
+    const int gpr = P.pitch / 4;
+    const long long ng = (long long)gpr * P.ny;
+    for (long long g = (long long)a.bid * kThreads + threadIdx.x; g < ng; g += (long long)a.nblk * kThreads) {
+        const int y = (int)(g / gpr), x0 = (int)(g % gpr) * 4;
+        if (x0 >= P.nx) continue;
+        const size_t i = (size_t)y * P.pitch + x0;
+        const float4 pv = *reinterpret_cast<const float4*>(p + i);
+        const float4 av = *reinterpret_cast<const float4*>(ap + i);
+        const float4 dv = *reinterpret_cast<const float4*>(dg + i);
+        float4 rv = *reinterpret_cast<const float4*>(r32 + i);
+        double2 xa = *reinterpret_cast<const double2*>(x + i), xb = *reinterpret_cast<const double2*>(x + i + 2);
+        float4 zv = *reinterpret_cast<const float4*>(z32 + i);
+        const float pp[4] = {pv.x, pv.y, pv.z, pv.w}, aa[4] = {av.x, av.y, av.z, av.w};
+        const float dd[4] = {dv.x, dv.y, dv.z, dv.w};
+        float rr4[4] = {rv.x, rv.y, rv.z, rv.w}, zz[4] = {zv.x, zv.y, zv.z, zv.w};
+        double xx[4] = {xa.x, xa.y, xb.x, xb.y};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            if (x0 + c >= P.nx) break;
+            const float r = __fmaf_rn(-af, aa[c], rr4[c]), z = __fdiv_rn(r, dd[c]);
+            xx[c] = xx[c] + alpha * (double)pp[c];
+            rr4[c] = r;
+            zz[c] = z;
             s0 += (double)r * (double)z;
             s1 += (double)r * (double)r;
         }
-        if (c.v1) {
-            const float r = __fmaf_rn(-af, ap1, r1), z = __fdiv_rn(r, d1);
-            x[c.i1] = x1 + alpha * (double)p1;
-            r32[c.i1] = r;
-            z32[c.i1] = z;
-            s0 += (double)r * (double)z;
-            s1 += (double)r * (double)r;
-        }
+        *reinterpret_cast<float4*>(r32 + i) = make_float4(rr4[0], rr4[1], rr4[2], rr4[3]);
+        *reinterpret_cast<float4*>(z32 + i) = make_float4(zz[0], zz[1], zz[2], zz[3]);
+        *reinterpret_cast<double2*>(x + i) = make_double2(xx[0], xx[1]);
+        *reinterpret_cast<double2*>(x + i + 2) = make_double2(xx[2], xx[3]);
     }
     double v[2] = {s0, s1};
     if (!red.reduce<2>(v, OPS2(kSum, kSum), kTagUpdate)) return false;

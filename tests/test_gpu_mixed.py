@@ -112,3 +112,24 @@ def test_batch_mixed_equals_single_mixed(gpu_lib):
         want = _run(w, "mixed", 8)
         for x, y in zip(g[:3], want[:3]):
             assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("nx,ny,front", [(37, 19, 6.0), (65, 33, 10.0), (3, 5, 2.0), (130, 70, 20.0)])
+def test_mixed_solve_ragged_domains(gpu_lib, port, nx, ny, front):
+    """The FP32 passes run over groups of four cells of a row: widths that are
+    not multiples of four (and the smallest domain) keep the FP64 bars against
+    the oracle with the same steps and rejections."""
+    from oracle import pyoracle
+    from pearl_gpu import workloads
+
+    n = 12
+    w = workloads.scaled(nx, ny, seed=3, front=front, undercooling=20.0, dt=4e-12, dt_max=8e-12)
+    phi, c, mu, s = _run(w, "mixed_solve", n)
+    po, co, muo = w.phi.copy(), w.carbon.copy(), w.mu.copy()
+    so = pyoracle.scalars_from(w.scalars)
+    rc, why, done, _ = port.advance_n(w.params, po, co, muo, so, n)
+    assert rc == 0 and done == n, why
+    assert s.rejected == so.rejected and s.time == so.time
+    assert np.abs(phi - po).max() <= 1e-10
+    assert np.abs(mu - muo).max() <= 1e-5
+    assert abs(c.sum() - co.sum()) <= 1e-12 * abs(co.sum())
