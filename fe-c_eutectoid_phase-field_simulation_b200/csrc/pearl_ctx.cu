@@ -616,6 +616,9 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
         per_sm = std::min(per_sm, n);
     }
     ctx->grid = std::max(1, std::min(per_sm * sms, ctx->P.ntiles));
+    // PEARL_GPU_GRID caps the block count (the grid-size sweeps of small domains)
+    if (const char* e = std::getenv("PEARL_GPU_GRID"))
+        if (std::atoi(e) > 0) ctx->grid = std::min(ctx->grid, std::atoi(e));
     // state: 2 x (3 phi + c + mu); work: K chi icpt diag x r z p0 p1 Ap  -> 20 planes
     const size_t pe = plane_elems(ctx);
     const int nplanes = 22;
