@@ -281,7 +281,7 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
     planes[kMapRc] = B.r;
     planes[kMapApc] = B.Ap;
     planes[kMapDiagc] = B.diag;
-    for (int m = 0; m < kMapCount; ++m) {
+    for (int m = 0; m < kMap32WE; ++m) {
         const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
         const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(double)};
         const bool tile_only = m >= kMapXc;
@@ -295,6 +295,21 @@ bool build_tensor_maps(pearl_gpu_ctx* ctx) {
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
+    }
+    // FP32 planes of the mixed solve, once pearl_gpu_set_precision has made them
+    if (B.wE32) {
+        float* planes32[6] = {B.wE32, B.wN32, B.z32, B.chi32, B.p32[0], B.p32[1]};
+        const TileGeometry g = tile_geometry(ctx->warps);
+        for (int m = kMap32WE; m < kMapCount; ++m) {
+            const cuuint64_t dims[2] = {(cuuint64_t)ctx->nx, (cuuint64_t)ctx->ny};
+            const cuuint64_t strides[1] = {(cuuint64_t)ctx->pitch * sizeof(float)};
+            const cuuint32_t box[2] = {(cuuint32_t)kBoxW32, (cuuint32_t)g.box_h};
+            const cuuint32_t estr[2] = {1, 1};
+            if (encode(&ctx->maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, planes32[m - kMap32WE], dims, strides, box,
+                       estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                       CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return false;
+        }
     }
     return true;
 }
@@ -703,6 +718,8 @@ int pearl_gpu_set_precision(pearl_gpu_ctx* ctx, int precision) {
             *pl = q;
             q += pe;
         }
+        // APPLY32 stages its FP32 planes through TMA like the FP64 passes
+        if (ctx->use_tma && !build_tensor_maps(ctx)) ctx->use_tma = false;
     }
     ctx->P.mixed = precision == PEARL_PRECISION_MIXED || precision == PEARL_PRECISION_MIXED_PROPOSE;
     ctx->P.mixed_cg = solve32 ? 1 : 0;

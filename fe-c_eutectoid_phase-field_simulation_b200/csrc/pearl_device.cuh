@@ -238,6 +238,9 @@ __device__ __forceinline__ double local_tau(const DevParams& P, double p0, doubl
 // the periodic x wrap is patched with plain loads and the y walls never read
 // their ghost row (the zero-flux faces are skipped or weighted by zero).
 constexpr int kBoxW = kTileX + 4;
+// FP32 boxes start four cells left of the tile (a 4-byte element's x must be a
+// multiple of four for a 16-byte aligned copy): columns 0..39 hold x0-4..x0+35.
+constexpr int kBoxW32 = kTileX + 8;
 constexpr int kMaxStageFields = 9;
 constexpr int kMaxStages = 4;
 
@@ -287,6 +290,8 @@ constexpr int kBoxH = kGeom.box_h;
 constexpr uint32_t kBoxBytes = kBoxW * kBoxH * sizeof(double);
 constexpr int kFieldStride = kGeom.field_stride;
 constexpr size_t kPipeDoubles = kGeom.pipe_doubles;
+// floats per staged FP32 field (128 B aligned)
+constexpr int kFieldStride32 = (int)(((size_t)kBoxW32 * kBoxH * sizeof(float) + 127) / 128 * 128 / sizeof(float));
 constexpr size_t kTmaSmemBytes = kGeom.tma_smem_bytes;
 constexpr int kMinBlocks = kGeom.min_blocks;
 }  // namespace PEARL_GEOM_NS
@@ -298,6 +303,9 @@ enum MapId : int {
     kMapK = 10, kMapChi, kMapIcpt, kMapX, kMapZ, kMapP0, kMapP1, kMapWE, kMapWN, kMapR, kMapAp, kMapDiag,
     // tile-only boxes (kTileX x kTileRows, no halo) for the pointwise CG update
     kMapXc, kMapP0c, kMapP1c, kMapRc, kMapApc, kMapDiagc,
+    // FP32 planes of the mixed solve's APPLY32 (encoded once the planes exist):
+    // kBoxW32 x box_h boxes starting four cells left of the tile
+    kMap32WE, kMap32WN, kMap32Z, kMap32Chi, kMap32P0, kMap32P1,
     kMapCount
 };
 
