@@ -70,8 +70,18 @@ extern "C" int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, 
     const long long nseg = (nsteps + K - 1) / K;
     const long long seglen = std::min(K, nsteps);
     const size_t n_ckpt = (size_t)(nseg + 1) * 5 * pe, n_tape = (size_t)seglen * 6 * pe, n_adj = 23 * pe;
-    double* slab = nullptr;
-    PG_CUDA(ctx, cudaMalloc(&slab, (n_ckpt + n_tape + n_adj + (size_t)nsteps + 8) * sizeof(double)));
+    // working memory is kept in the context and grown when a call needs more, so
+    // repeated gradients of one domain allocate once (a fresh cudaMalloc of
+    // hundreds of MB per call cost up to 0.35 s of host time)
+    const size_t need = n_ckpt + n_tape + n_adj + (size_t)nsteps + 8;
+    if (ctx->adj_slab_elems < need) {
+        if (ctx->adj_slab) cudaFree(ctx->adj_slab);
+        ctx->adj_slab = nullptr;
+        ctx->adj_slab_elems = 0;
+        PG_CUDA(ctx, cudaMalloc(&ctx->adj_slab, need * sizeof(double)));
+        ctx->adj_slab_elems = need;
+    }
+    double* const slab = ctx->adj_slab;
     double* ckpt = slab;
     double* tape = ckpt + n_ckpt;
     double* adj = tape + n_tape;
@@ -214,7 +224,6 @@ extern "C" int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, 
     }
     cudaStreamSynchronize(ctx->stream);
     for (auto& ev : e) cudaEventDestroy(ev);
-    cudaFree(slab);
     return rc;
 }
 

@@ -200,14 +200,15 @@ int launch(pearl_gpu_ctx* ctx, KArgs& args) {
     args.B = ctx->B;
     void* kargs[] = {&args};
     PG_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    args.use_tma = ctx->use_tma ? 1 : 0;
-    if (ctx->use_tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
+    const bool tma = ctx->use_tma && ctx->stage_tma;
+    args.use_tma = tma ? 1 : 0;
+    if (tma) std::memcpy(args.maps, ctx->maps, sizeof ctx->maps);
     const TileGeometry g = tile_geometry(ctx->warps);
     // the mixed-solve kernel holds only the run mode
     const bool solve32 = ctx->P.mixed_cg != 0 && args.mode == kModeRun;
     PG_CUDA(ctx, cudaLaunchCooperativeKernel(step_kernel(ctx->warps, solve32), dim3(ctx->grid),
                                              dim3(g.threads), kargs,
-                                             ctx->use_tma ? g.tma_smem_bytes : 0, ctx->stream));
+                                             tma ? g.tma_smem_bytes : 0, ctx->stream));
     ctx->launches++;
     PG_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     rc = pull_ctl(ctx);
@@ -637,6 +638,13 @@ int pearl_gpu_create(const pearl_params* params, int nx, int ny, int device, pea
     // PEARL_GPU_GRID caps the block count (the grid-size sweeps of small domains)
     if (const char* e = std::getenv("PEARL_GPU_GRID"))
         if (std::atoi(e) > 0) ctx->grid = std::min(ctx->grid, std::atoi(e));
+    // TMA staging pays once a block has a few tiles per pass to pipeline; with
+    // fewer, the pipeline's fill and proxy fences cost more than plain loads
+    // (1965 MHz, one GPU: 768x1024, 5.2 tiles a block, 0.258 staged against
+    // 0.234 ms/step plain; 1024x1024, 6.9 tiles, 0.300 against 0.304;
+    // 1024x2048, 13.8 tiles, 0.497 against 0.601; 256x512 0.0947 against
+    // 0.0733).  PEARL_GPU_TMA=1 stages whatever the size, =0 never.
+    ctx->stage_tma = ctx->use_tma && ((tma_env && std::atoi(tma_env) != 0) || ctx->P.ntiles >= 6LL * ctx->grid);
     // state: 2 x (3 phi + c + mu); work: K chi icpt diag x r z p0 p1 Ap  -> 20 planes
     const size_t pe = plane_elems(ctx);
     const int nplanes = 22;
@@ -688,6 +696,7 @@ void pearl_gpu_destroy(pearl_gpu_ctx* ctx) {
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->d_fill) cudaFree(ctx->d_fill);
     if (ctx->slab32) cudaFree(ctx->slab32);
+    if (ctx->adj_slab) cudaFree(ctx->adj_slab);
     if (ctx->d_hist) cudaFree(ctx->d_hist);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);

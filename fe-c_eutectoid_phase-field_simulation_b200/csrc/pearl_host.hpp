@@ -22,7 +22,8 @@ struct NvtxRange {
 struct pearl_gpu_ctx {
     CUtensorMap maps[pearl_gpu::kMapCount];
     int warps = 8;  // block shape of the context's kernels: 8 or 16 warps (pearl_gpu::tile_geometry)
-    bool use_tma = false;
+    bool use_tma = false;     // tensor maps built and shared memory granted (batches reuse the maps)
+    bool stage_tma = false;   // this context's launches stage through TMA (see the size rule at create)
     int device = 0;
     int nx = 0, ny = 0, pitch = 0;
     cudaStream_t stream = nullptr;
@@ -40,6 +41,8 @@ struct pearl_gpu_ctx {
     double last_ms = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int adj_grid = 0;  // cooperative grid of the adjoint kernel (0 until first use)
+    double* adj_slab = nullptr;  // the adjoint's checkpoints, tape and planes, kept for later calls
+    size_t adj_slab_elems = 0;
     pearl_step_info* d_hist = nullptr;  // per-step history ring (pearl_gpu_set_history)
     void* d_fill = nullptr;             // filling commands of pearl_gpu_fill (PEARL_FILL_MAX_OPS)
     long long hist_cap = 0, hist_count = 0;

@@ -361,7 +361,9 @@ typedef struct pearl_adjoint_report {
     double forward_ms, recompute_ms, adjoint_ms; /* device time of the three sweeps */
 } pearl_adjoint_report;
 
-/* target_alpha[y*nx+x] on the host. */
+/* target_alpha[y*nx+x] on the host.  The checkpoints, tape and adjoint
+ * planes stay allocated in the context for later calls (grown when a call
+ * needs more) and are freed by pearl_gpu_destroy. */
 int pearl_gpu_adjoint_gradient(pearl_gpu_ctx* ctx, long long nsteps, int checkpoint_every,
                                const double* target_alpha, pearl_adjoint_report* out);
 

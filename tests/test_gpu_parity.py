@@ -31,9 +31,19 @@ def _ctx(w):
 SIZES = [(64, 48, 12.0), (37, 19, 6.0), (137, 250, 40.0), (128, 256, 32.0)]
 
 
+# Contexts stage tiles through TMA only when every block has several tiles a
+# pass (the small domains here run on plain loads by default); PEARL_GPU_TMA=1
+# forces the staged path, so both paths meet the same bars.
+STAGING = ["default", "1"]
+
+
+@pytest.mark.parametrize("staging", STAGING)
 @pytest.mark.parametrize("nx,ny,front", SIZES)
-def test_propose_phi_bitwise(gpu_lib, port, nx, ny, front):
+def test_propose_phi_bitwise(gpu_lib, port, monkeypatch, staging, nx, ny, front):
     from pearl_gpu import workloads
+
+    if staging != "default":
+        monkeypatch.setenv("PEARL_GPU_TMA", staging)
 
     w = workloads.scaled(nx, ny, seed=3, front=front, jitter=0.1, front_jitter=1)
     with _ctx(w) as ctx:
@@ -107,9 +117,13 @@ def _compare_run(ctx, w, port, nsteps, forced=None):
     return infos, oinfos
 
 
-def test_advance_small_fixed_dt(gpu_lib, port):
+@pytest.mark.parametrize("staging", STAGING)
+def test_advance_small_fixed_dt(gpu_lib, port, monkeypatch, staging):
     """128x256, 4 pairs, fixed dt 4e-12 s: 25 accepted steps (includes a rejected attempt)."""
     from pearl_gpu import workloads
+
+    if staging != "default":
+        monkeypatch.setenv("PEARL_GPU_TMA", staging)
 
     w = workloads.plain_small()
     with _ctx(w) as ctx:
@@ -191,12 +205,17 @@ def test_run_matches_advance(gpu_lib):
 EDGE_SIZES = [(3, 2, 1.0), (3, 5, 2.0), (4, 3, 1.5), (31, 17, 6.0), (33, 16, 8.0), (65, 33, 10.0)]
 
 
+@pytest.mark.parametrize("staging", STAGING)
 @pytest.mark.parametrize("nx,ny,front", EDGE_SIZES)
-def test_smallest_and_ragged_domains(gpu_lib, port, nx, ny, front):
+def test_smallest_and_ragged_domains(gpu_lib, port, monkeypatch, staging, nx, ny, front):
     """The smallest domains the reference accepts (nx >= 3, ny >= 2) and widths
     and heights just off the 32x16 tile: propose_phi bitwise, then 8 coupled
-    steps against the oracle with the same decisions."""
+    steps against the oracle with the same decisions; on plain loads (the
+    default at these sizes) and staged through TMA."""
     from pearl_gpu import workloads
+
+    if staging != "default":
+        monkeypatch.setenv("PEARL_GPU_TMA", staging)
 
     w = workloads.scaled(nx, ny, seed=3, front=front)
     with _ctx(w) as ctx:
