@@ -1,8 +1,8 @@
 /*
  * pearl_adjoint.c — CPU reference gradient of the Pearl time step.
  *
- * TEST INFRASTRUCTURE ONLY (same rules as pearl_oracle.c): the checker of the
- * device adjoint, never part of the product.
+ * TEST INFRASTRUCTURE ONLY (same rules as pearl_oracle.c): what the device
+ * adjoint is compared against, never part of the product.
  *
  * The reference has no adjoint.  This file differentiates the discrete step
  * of pearl_oracle.c (itself bit-identical to pearl_serial.cpp) by hand:

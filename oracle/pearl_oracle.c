@@ -2,7 +2,8 @@
  * pearl_oracle.c — CPU restatement of the Pearl hot path (TEST INFRASTRUCTURE).
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
- * this file, as the checker or as the timed CPU port; the product never does.
+ * this file, as the reference results are compared against or as the timed
+ * CPU port; the product never does.
  * Each function restates the reference pearl_serial.cpp (cited file:line)
  * with the same operation order and sequential reductions.  It is compiled
  * with -ffp-contract=off so that, like the reference built for plain x86-64,

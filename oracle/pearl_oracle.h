@@ -2,8 +2,8 @@
  * pearl_oracle — CPU restatement of the Pearl time-step hot path.
  *
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
- * bench's CPU-baseline leg may load this library, and only as the checker
- * (or as the timed CPU port).  The product (libpearl_gpu.so, pearl_gpu)
+ * bench's CPU-baseline leg may load this library, and only as the reference
+ * results are compared against (or as the timed CPU port).  The product (libpearl_gpu.so, pearl_gpu)
  * never links or calls it.
  *
  * Every function restates the algorithm of the reference file
