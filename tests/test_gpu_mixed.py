@@ -133,3 +133,21 @@ def test_mixed_solve_ragged_domains(gpu_lib, port, nx, ny, front):
     assert np.abs(phi - po).max() <= 1e-10
     assert np.abs(mu - muo).max() <= 1e-5
     assert abs(c.sum() - co.sum()) <= 1e-12 * abs(co.sum())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed_solve", "mixed"])
+def test_staged_and_plain_paths_agree_bitwise(gpu_lib, monkeypatch, precision):
+    """The phases read their tiles either staged through TMA (FP64 and FP32
+    boxes) or straight from the planes; the arithmetic and the tile owners are
+    the same, so a run gives the same bits either way (a ragged domain, forced
+    both ways: by default a domain this small is not staged)."""
+    from pearl_gpu import workloads
+
+    w = workloads.scaled(130, 70, seed=3, front=20.0, undercooling=20.0, dt=4e-12, dt_max=8e-12)
+    monkeypatch.setenv("PEARL_GPU_TMA", "1")
+    staged = _run(w, precision, 12)
+    monkeypatch.setenv("PEARL_GPU_TMA", "0")
+    plain = _run(w, precision, 12)
+    for a, b in zip(staged[:3], plain[:3]):
+        assert np.array_equal(a, b)
+    assert staged[3].time == plain[3].time and staged[3].rejected == plain[3].rejected
