@@ -99,7 +99,8 @@ def workload(nx: int, ny: int, seed: int = 0):
 
 def config_dict(w, args) -> dict:
     return {
-        "workload": f"plain FP64 large: {w.nx}x{w.ny} (x periodic, y growth), 64 pairs spacing 32+-10%, "
+        "workload": f"plain FP64 large: {w.nx}x{w.ny} (x periodic, y growth), {max(1, w.nx // 32)} pairs "
+                    f"spacing 32+-10%, "
                     f"f_alpha 0.875, T_E-20K, adaptive dt, moving window, implicit diffusion",
         "nx": w.nx, "ny": w.ny, "cells": w.cells, "dx_m": w.params["dx"],
         "dt": w.params["dt_max"] / 2, "dt_max": w.params["dt_max"],
